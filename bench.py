@@ -1,0 +1,315 @@
+#!/usr/bin/env python3
+"""Throughput benchmark: decomposed nodes/s of the IVM branch-and-bound on the
+50-job x 20-machine instance (U[1,99], seed 2), weak bound refined by the
+Johnson two-machine bound (boundingMode 2), MinMin branching, initial upper
+bound from NEH, 65536 explorers.
+
+A step is one exploration window of `--window` seconds of device time on the
+resident search (the tree is far too large to finish; the search continues
+across steps).  `value` = decomposed nodes in the K timed steps / their
+CUDA-event time, summed over ranks, time = max over ranks.  `e2e` is the same
+metric through the C ABI from host memory: engine creation (instance upload
+and table build), root + unfold, one window, result read-back, destroy.
+
+  python bench.py [--gpus N] [--steps K] [--warmup W] [--window S] [--impl reference]
+
+Under torchrun each rank explores its own slice of the permutation space
+(factoradic sub-interval of the root level) and the ranks exchange the best
+makespan (a 4-byte MIN all-reduce) between windows.
+"""
+import argparse
+import json
+import os
+import statistics
+import subprocess
+import sys
+import tempfile
+import time
+
+ROOT = os.path.dirname(os.path.abspath(__file__))
+sys.path.insert(0, ROOT)
+
+N_JOBS, N_MACH, SEED = 50, 20, 2
+NB_IVMS = 65536
+BOUND_MODE, BRANCH_MODE = 2, 3
+METRIC = "decomposed nodes/s (50x20, Johnson LB)"
+
+
+def parse():
+    ap = argparse.ArgumentParser()
+    ap.add_argument("--gpus", type=int, default=1)
+    ap.add_argument("--steps", type=int, default=10)
+    ap.add_argument("--warmup", type=int, default=3)
+    ap.add_argument("--window", type=float, default=6.0)
+    ap.add_argument("--impl", default="ours", choices=["ours", "reference"])
+    ap.add_argument("--e2e-steps", type=int, default=2)
+    ap.add_argument("--cpu-sample", type=float, default=15.0)
+    return ap.parse_args()
+
+
+def dist_env():
+    ws = int(os.environ.get("WORLD_SIZE", "1"))
+    rank = int(os.environ.get("RANK", "0"))
+    local = int(os.environ.get("LOCAL_RANK", "0"))
+    return ws, rank, local
+
+
+def workload_config(extra=None):
+    cfg = {"workload": "pfsp-50x20-u1-99-seed2", "n_jobs": N_JOBS, "n_machines": N_MACH, "seed": SEED,
+           "bounding_mode": BOUND_MODE, "branching_mode": BRANCH_MODE, "nb_ivms": NB_IVMS,
+           "initial_ub": "NEH", "l2": "explorer state (65536 x 4.3 KB) exceeds L2; no flush"}
+    if extra:
+        cfg.update(extra)
+    return cfg
+
+
+# ---------------------------------------------------------------------------
+# CPU baseline: the reference multicore B&B (oracle/_ref/bbJ) on the host cores
+# ---------------------------------------------------------------------------
+def reference_cpu_run(p, ub, seconds, threads=0):
+    """One bounded run of the reference's own multicore B&B; returns
+    (nodes/s, nodes, walltime, threads)."""
+    import oracle
+    if not oracle.reference_available():
+        return None
+    r = oracle.run_reference_bb(p, ub=ub, bound_mode=BOUND_MODE, branch_mode=BRANCH_MODE, threads=threads,
+                                johnson=True, time_limit=seconds, timeout=seconds * 4 + 120)
+    if "decomposed" not in r or not r.get("walltime"):
+        return None
+    return r["decomposed"] / r["walltime"], r["decomposed"], r["walltime"]
+
+
+def host_cores():
+    return os.cpu_count() or 1
+
+
+# ---------------------------------------------------------------------------
+# clocks during the timed region
+# ---------------------------------------------------------------------------
+class ClockSampler:
+    QUERY = ("index,clocks.sm,clocks.max.sm,power.draw,clocks_event_reasons.active,"
+             "clocks_event_reasons.hw_slowdown,clocks_event_reasons.hw_thermal_slowdown,"
+             "clocks_event_reasons.sw_thermal_slowdown,clocks_event_reasons.sw_power_cap")
+
+    def __init__(self, index):
+        self.index = index
+        self.proc = None
+        self.path = None
+
+    def __enter__(self):
+        fd, self.path = tempfile.mkstemp(prefix="clocks_", suffix=".csv")
+        os.close(fd)
+        try:
+            self.proc = subprocess.Popen(["nvidia-smi", "-i", str(self.index), "--query-gpu=" + self.QUERY,
+                                          "--format=csv,noheader,nounits", "-lms", "200"],
+                                         stdout=open(self.path, "w"), stderr=subprocess.DEVNULL)
+        except OSError:
+            self.proc = None
+        return self
+
+    def __exit__(self, *a):
+        if self.proc:
+            self.proc.terminate()
+            try:
+                self.proc.wait(timeout=5)
+            except subprocess.TimeoutExpired:
+                self.proc.kill()
+
+    def summary(self):
+        rows = []
+        try:
+            for line in open(self.path):
+                f = [x.strip() for x in line.split(",")]
+                if len(f) >= 9 and f[1].isdigit():
+                    rows.append(f)
+        except OSError:
+            pass
+        finally:
+            if self.path and os.path.exists(self.path):
+                os.unlink(self.path)
+        if not rows:
+            return {"sm_mhz": None, "sm_max_mhz": None, "reasons": ["unavailable"]}
+        sm = [int(r[1]) for r in rows]
+        names = ["hw_slowdown", "hw_thermal_slowdown", "sw_thermal_slowdown", "sw_power_cap"]
+        reasons = sorted({names[i] for r in rows for i in range(4) if r[5 + i].lower() == "active"})
+        return {"sm_mhz": statistics.median(sm), "sm_max_mhz": int(rows[0][2]), "reasons": reasons,
+                "samples": len(rows)}
+
+
+# ---------------------------------------------------------------------------
+# factoradic slices of the permutation space, one per rank
+# ---------------------------------------------------------------------------
+def rank_slice(n, rank, world):
+    """(pos, end) factoradic vectors of rank's share of the first level:
+    the n root cells are split into contiguous blocks, one per rank."""
+    if world == 1:
+        return None
+    per = [n // world + (1 if r < n % world else 0) for r in range(world)]
+    lo = sum(per[:rank])
+    hi = lo + per[rank] - 1
+    if per[rank] == 0:
+        return None
+    pos = [lo] + [0] * (n - 1)
+    end = [hi] + [n - 1 - i for i in range(1, n)]
+    return pos, end
+
+
+def run_ours(args):
+    import numpy as np
+    import torch
+    import pbbperm_b200 as pb
+
+    ws, rank, local = dist_env()
+    torch.cuda.set_device(local)
+    dist = None
+    if ws > 1:
+        import torch.distributed as dist
+        from datetime import timedelta
+        dist.init_process_group("nccl", timeout=timedelta(seconds=300))
+    p = pb.synthetic_instance(SEED, N_JOBS, N_MACH)
+    ub, _ = pb.neh(p)
+    cfg = pb.Config(boundingMode=BOUND_MODE, adaptiveBranchingMode=BRANCH_MODE, nbIVMs=NB_IVMS, device=local)
+    eng = pb.Engine(p, cfg)
+    sl = rank_slice(N_JOBS, rank, ws)
+    if sl is None:
+        eng.start(ub=ub)
+    else:
+        eng.start_interval(ub=ub, pos=sl[0], end=sl[1])
+
+    def window():
+        t0 = eng.result()
+        done = eng.explore(args.window)
+        t1 = eng.result()
+        return t1["decomposed"] - t0["decomposed"], t1["device_seconds"] - t0["device_seconds"], done, t1
+
+    def exchange_ub(res):
+        if dist is None:
+            return
+        t = torch.tensor([res["cost"]], dtype=torch.int32, device="cuda")
+        dist.all_reduce(t, op=dist.ReduceOp.MIN)
+        eng.set_ub(int(t.item()))
+
+    for _ in range(args.warmup):
+        _, _, _, res = window()
+        exchange_ub(res)
+    torch.cuda.synchronize()
+    if dist:
+        dist.barrier()
+    nodes = 0
+    dev_s = 0.0
+    launches = 0
+    steps_done = 0
+    with ClockSampler(local) as clk:
+        wall0 = time.perf_counter()
+        for _ in range(args.steps):
+            dn, ds, done, res = window()
+            nodes += dn
+            dev_s += ds
+            launches += 2          # explorer kernel + queue re-arm kernel
+            steps_done += 1
+            exchange_ub(res)
+        torch.cuda.synchronize()
+        wall = time.perf_counter() - wall0
+    if dist:
+        dist.barrier()
+    clocks = clk.summary()
+    res = eng.result()
+    kern = eng.kernel_stats()
+    eng.close()
+
+    # whole-job aggregate: nodes summed, time = max over ranks
+    tot_nodes, max_s = nodes, dev_s
+    if dist:
+        t = torch.tensor([float(nodes), dev_s], dtype=torch.float64, device="cuda")
+        a = t.clone()
+        dist.all_reduce(a[:1], op=dist.ReduceOp.SUM)
+        b = t[1:].clone()
+        dist.all_reduce(b, op=dist.ReduceOp.MAX)
+        tot_nodes, max_s = a[0].item(), b[0].item()
+    value = tot_nodes / max_s if max_s > 0 else 0.0
+
+    out = None
+    if rank == 0:
+        # e2e through the C ABI from host buffers (rank 0 measures; all ranks would do the same work)
+        e2e_vals = []
+        for _ in range(args.e2e_steps):
+            t0 = time.perf_counter()
+            with pb.Engine(p, cfg) as e2:
+                r2 = e2.solve(ub=ub, time_limit=args.window)
+            el = time.perf_counter() - t0
+            e2e_vals.append(r2["decomposed"] / el)
+        h2d = int(p.size * 4 + N_JOBS * 192 * 8 + 2 * 192 + 2 * N_MACH * 4 + 4 + 64 * 4)
+        d2h = int(160 + 4 * max(1, int(args.window / 2.0 + 0.999)) + 64)
+        e2e = {"value": statistics.median(e2e_vals) * ws, "unit": "nodes/s", "h2d_bytes_per_step": h2d,
+               "d2h_bytes_per_step": d2h}
+
+        # roofline of the explorer kernel: INT32 work of the bound formulation per second
+        peak = pb.int32_peak(local)
+        ops = kern["int32_ops"]
+        achieved = ops / kern["device_seconds"] / 1e9 if kern["device_seconds"] > 0 else 0.0
+        roofline = {"bound": "int32", "achieved": round(achieved, 1), "peak": round(peak, 1), "unit": "Gop/s",
+                    "frac": round(achieved / peak, 4) if peak else None, "traffic": None,
+                    "peak_source": "measured: pbb_diag_int32_peak (IADD+IMNMX register chains, all SMs)",
+                    "work_model": kern["work_model"]}
+        cpu = None
+        if ws == 1:
+            r = reference_cpu_run(p, ub, args.cpu_sample)
+            if r:
+                cpu = {"value": round(r[0], 1), "unit": "nodes/s", "cores": host_cores(), "kind": "reference",
+                       "sample": "oracle/_ref/bbJ (reference multicore, Johnson call restored) on the same "
+                                 "instance/UB/modes, threads = all host cores, %.0f s window" % args.cpu_sample}
+        out = {"metric": METRIC, "value": round(value, 1), "unit": "nodes/s", "n_gpus": ws, "steps": steps_done,
+               "warmup": args.warmup, "ms_per_step": round(max_s / max(1, steps_done) * 1e3, 3),
+               "higher_is_better": True, "scaling": "weak", "vs_baseline": None, "dtype": "int32",
+               "data": "synthetic (seeded splitmix64 U[1,99])",
+               "config": workload_config({"window_s": args.window, "parallelism": "dp%d" % ws if ws > 1 else "single"}),
+               "e2e": e2e, "gpu_launches": launches, "clocks": clocks, "roofline": roofline,
+               "cpu_baseline": cpu, "wall_s": round(wall, 3), "best_makespan": res["cost"],
+               "counters": {"decomposed": res["decomposed"], "johnson_bounds": res["johnson_bounds"],
+                            "simple_bounds": res["simple_bounds"], "leaves": res["leaves"],
+                            "steals": res["steals"]}}
+    if dist:
+        dist.barrier()
+        dist.destroy_process_group()
+    if out:
+        print(json.dumps(out), flush=True)
+
+
+def run_reference(args):
+    ws, rank, _ = dist_env()
+    if rank != 0:
+        return
+    import oracle
+    from pbbperm_b200.instances import synthetic_instance
+    if not oracle.reference_available():
+        print(json.dumps({"impl": "reference", "unavailable": "oracle/_ref not built (python oracle/build_ref.py)"}))
+        return
+    p = synthetic_instance(SEED, N_JOBS, N_MACH)
+    ub, _ = oracle.Oracle(p).neh()
+    step_s = min(args.window, 8.0)
+    for _ in range(args.warmup):
+        reference_cpu_run(p, ub, 2.0)
+    vals = []
+    t0 = time.perf_counter()
+    for _ in range(args.steps):
+        r = reference_cpu_run(p, ub, step_s)
+        if r:
+            vals.append(r[0])
+    wall = time.perf_counter() - t0
+    value = statistics.median(vals) if vals else 0.0
+    out = {"impl": "reference", "metric": METRIC, "value": round(value, 1), "unit": "nodes/s", "n_gpus": ws,
+           "steps": args.steps, "warmup": args.warmup, "ms_per_step": round(wall / max(1, args.steps) * 1e3, 3),
+           "higher_is_better": True, "scaling": "weak", "vs_baseline": None, "dtype": "int32",
+           "data": "synthetic (seeded splitmix64 U[1,99])", "config": workload_config({"window_s": step_s}),
+           "cpu_baseline": {"value": round(value, 1), "unit": "nodes/s", "cores": host_cores(), "kind": "reference",
+                            "sample": "oracle/_ref/bbJ, all host threads, %.0f s window per step" % step_s},
+           "e2e": {"value": round(value, 1), "unit": "nodes/s", "h2d_bytes_per_step": 0, "d2h_bytes_per_step": 0}}
+    print(json.dumps(out), flush=True)
+
+
+if __name__ == "__main__":
+    a = parse()
+    if a.impl == "reference":
+        run_reference(a)
+    else:
+        run_ours(a)

@@ -1,0 +1,134 @@
+/*
+ * pbbperm.h -- C ABI of the B200 IVM branch-and-bound engine for the
+ * permutation flow-shop (makespan).  Plain pointers and sizes only; every call
+ * returns a status code (PBB_OK or a negative PBB_E_*), never exits.
+ *
+ * Reference interfaces each entry point stands in for (jangmys/PBBPerm):
+ *   pbb_engine_create   gpubb::gpubb + initialize + initializeBoundFSP + copyH2D
+ *                       (gpu/include/gpubb.h:103-228, gpu/src/gpubb.cu:24-116,
+ *                       :826-1060), instance from instance_abstract
+ *                       (bounds/include/instance_abstract.h:6-9)
+ *   pbb_solve           gpubb::initFullInterval + next + getStats
+ *                       (gpubb.h:113,237,245; gpu/src/main.cpp:52-69) and the
+ *                       statistics printed by pbab::printStats (common/src/pbab.cpp:40-74)
+ *   pbb_start / pbb_explore / pbb_get_result
+ *                       the same loop in resumable windows (gpubb::next(int&,int&),
+ *                       gpubb.h:238; matrix_controller::interruptExploration
+ *                       multicore/src/matrix_controller.cpp:459-462)
+ *   pbb_bound_children  bound_abstract::boundChildren + bornes_calculer
+ *                       (bounds/include/bound_abstract.h:15-26) for a batch of nodes
+ *   pbb_neh             fastNEH::runNEH initial upper bound (heuristic/src/fastNEH.cpp:230-243)
+ *   pbb_engine_destroy  gpubb::~gpubb (gpubb.h:104)
+ */
+#ifndef PBBPERM_H
+#define PBBPERM_H
+
+#include <stdint.h>
+
+#ifdef __cplusplus
+extern "C" {
+#endif
+
+#define PBB_OK 0
+#define PBB_E_INVAL (-1)       /* bad argument or unsupported instance/config */
+#define PBB_E_NOMEM (-2)       /* device allocation failed */
+#define PBB_E_CUDA (-3)        /* CUDA runtime error (message in pbb_last_error) */
+#define PBB_E_TIMEOUT (-4)     /* a device wait ran out of its bound */
+#define PBB_E_UNSUPPORTED (-5) /* option the engine does not implement */
+
+#define PBB_MAX_JOBS 64
+#define PBB_MAX_MACHINES 32
+
+/* Instance: n_jobs x n_machines processing times, row-major machine-major
+ * (p[k * n_jobs + j] = time of job j on machine k), the order of the
+ * reference's instance stream (bounds/src/instance_flowshop.cpp:91-101). */
+typedef struct pbb_instance {
+    int32_t n_jobs;
+    int32_t n_machines;
+    const int32_t* p;
+} pbb_instance;
+
+/* Search settings; field names follow the reference ini keys
+ * (common/src/arguments.cpp:80-132). */
+typedef struct pbb_config {
+    int32_t bounding_mode;      /* [bb] boundingMode: 0 weak, 1 Johnson, 2 weak then Johnson */
+    int32_t branching_mode;     /* [bb] adaptiveBranchingMode (CPU numbering): -3,-2,-1,1,2,3 */
+    int32_t find_all;           /* [bb] findAll */
+    int32_t johnson_mode;       /* [bb] JohnsonMode: 0 all pairs, 1 (k,m), 2 (k,k+1) */
+    int32_t early_stop_johnson; /* [bb] earlyStopJohnson: must be 0 */
+    int32_t sorted_dfs;         /* [bb] sortedDFS: must be 0 */
+    int32_t nb_ivms;            /* [gpu] nbIVMs: explorers */
+    int32_t device;             /* CUDA device ordinal */
+    int32_t warps_per_cta;      /* 0 = largest that fits shared memory */
+    int32_t ctas;               /* 0 = SMs x resident CTAs per SM */
+} pbb_config;
+
+typedef struct pbb_stats {
+    uint64_t decomposed;        /* TOTdecomposed */
+    uint64_t johnson_bounds;    /* TOTjohnson LBs */
+    uint64_t simple_bounds;     /* TOTsimple LBs */
+    uint64_t leaves;            /* TOTleaves */
+    uint64_t steals;            /* intervals handed between explorers */
+} pbb_stats;
+
+typedef struct pbb_result {
+    int32_t complete;           /* 1: the whole search space was explored */
+    int32_t found;              /* 1: a leaf improved the initial bound ("Found optimal solution") */
+    int32_t cost;               /* best makespan known (the initial bound if not improved) */
+    int32_t n_jobs;
+    int32_t perm[PBB_MAX_JOBS]; /* best permutation when found */
+    pbb_stats stats;
+    double device_seconds;      /* device time of the exploration kernels */
+} pbb_result;
+
+typedef struct pbb_engine pbb_engine;
+
+void pbb_config_default(pbb_config* cfg);
+const char* pbb_last_error(void);
+
+int pbb_engine_create(const pbb_instance* inst, const pbb_config* cfg, pbb_engine** out);
+int pbb_engine_destroy(pbb_engine* e);
+
+/* Solve to completion or until time_limit_s (<= 0: no limit) with initial
+ * upper bound `ub` (INT32_MAX = +inf) and root row `root_perm` (NULL =
+ * identity).  Leaves with cost < ub (<= with find_all) improve the bound. */
+int pbb_solve(pbb_engine* e, int32_t ub, const int32_t* root_perm, double time_limit_s, pbb_result* out);
+
+/* Resumable form: pbb_start bounds the root and unfolds the first path;
+ * each pbb_explore runs the explorers for up to `seconds` of device time and
+ * sets *done when the search space is exhausted. */
+int pbb_start(pbb_engine* e, int32_t ub, const int32_t* root_perm);
+int pbb_explore(pbb_engine* e, double seconds, int32_t* done);
+
+/* Start on the factoradic interval [pos, end] (n digits each, digit i in
+ * [0, n-i)): gpubb::initAtInterval / initFromFac (gpu/include/gpubb.h:232,248),
+ * sequentialbb::initAtInterval (multicore/src/sequentialbb.cpp:84-106). */
+int pbb_start_interval(pbb_engine* e, int32_t ub, const int32_t* root_perm, const int32_t* pos, const int32_t* end);
+
+/* Lower the incumbent to `ub` (a bound found by another solver; no
+ * permutation is attached): solution::updateCost (common/src/solution.cpp:48-58). */
+int pbb_set_ub(pbb_engine* e, int32_t ub);
+int pbb_get_result(pbb_engine* e, pbb_result* out);
+
+/* Children bounds of `count` nodes of one instance.  Node i is the schedule
+ * sched[i*n .. i*n+n) with jobs [0..limit1[i]] fixed in front and
+ * [limit2[i]..n) fixed at the back.  Per job id (0 for fixed jobs):
+ * weak LB of the child with the job appended at the front / back
+ * (bound_fsp_weak::boundChildren) and Johnson LB of the same children
+ * (bound_fsp_strong::bornes_calculer on the child, no early exit).  Per node:
+ * its own weak and Johnson LB (bornes_calculer); with at most one free job the
+ * Johnson value is the makespan of the schedule as given.  Output arrays may
+ * be NULL when not wanted. */
+int pbb_bound_children(const pbb_instance* inst, int32_t johnson_mode, int32_t device, int32_t count,
+                       const int32_t* sched, const int32_t* limit1, const int32_t* limit2,
+                       int32_t* weak_begin, int32_t* weak_end, int32_t* strong_begin, int32_t* strong_end,
+                       int32_t* node_weak, int32_t* node_strong);
+
+/* NEH upper bound: jobs by decreasing total time, each inserted at the first
+ * position of least partial makespan (host code). */
+int pbb_neh(const pbb_instance* inst, int32_t* perm, int32_t* cost);
+
+#ifdef __cplusplus
+}
+#endif
+#endif

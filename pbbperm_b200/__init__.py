@@ -1,0 +1,263 @@
+"""B200 IVM branch-and-bound for the permutation flow-shop (makespan).
+
+Host-side mirror of the reference's engine and bounds interfaces over the C
+ABI of libpbbperm.so (include/pbbperm.h):
+
+  Engine         gpubb (gpu/include/gpubb.h): create / solve / start / explore
+  bound_children bound_abstract::boundChildren + bornes_calculer
+                 (bounds/include/bound_abstract.h) for a batch of nodes
+  neh            fastNEH::runNEH initial upper bound
+  Config         the reference's ini keys (common/src/arguments.cpp:80-132)
+
+All compute runs in CUDA kernels; there is no CPU fallback.  Loading fails
+loudly when the native library is missing.
+"""
+import ctypes
+import os
+
+import numpy as np
+
+from .instances import synthetic_instance, read_vrf, write_vrf  # noqa: F401
+
+PKG = os.path.dirname(os.path.abspath(__file__))
+LIB_PATH = os.path.join(PKG, "libpbbperm.so")
+
+PBB_OK = 0
+PBB_E_INVAL = -1
+PBB_E_NOMEM = -2
+PBB_E_CUDA = -3
+PBB_E_TIMEOUT = -4
+PBB_E_UNSUPPORTED = -5
+MAX_JOBS = 64
+INF = 2**31 - 1
+
+_i32p = ctypes.POINTER(ctypes.c_int32)
+
+
+class PbbError(RuntimeError):
+    def __init__(self, code, msg):
+        super().__init__("pbbperm error %d: %s" % (code, msg))
+        self.code = code
+
+
+class _Instance(ctypes.Structure):
+    _fields_ = [("n_jobs", ctypes.c_int32), ("n_machines", ctypes.c_int32), ("p", _i32p)]
+
+
+class _Config(ctypes.Structure):
+    _fields_ = [("bounding_mode", ctypes.c_int32), ("branching_mode", ctypes.c_int32),
+                ("find_all", ctypes.c_int32), ("johnson_mode", ctypes.c_int32),
+                ("early_stop_johnson", ctypes.c_int32), ("sorted_dfs", ctypes.c_int32),
+                ("nb_ivms", ctypes.c_int32), ("device", ctypes.c_int32),
+                ("warps_per_cta", ctypes.c_int32), ("ctas", ctypes.c_int32)]
+
+
+class _Stats(ctypes.Structure):
+    _fields_ = [("decomposed", ctypes.c_uint64), ("johnson_bounds", ctypes.c_uint64),
+                ("simple_bounds", ctypes.c_uint64), ("leaves", ctypes.c_uint64),
+                ("steals", ctypes.c_uint64)]
+
+
+class _Result(ctypes.Structure):
+    _fields_ = [("complete", ctypes.c_int32), ("found", ctypes.c_int32), ("cost", ctypes.c_int32),
+                ("n_jobs", ctypes.c_int32), ("perm", ctypes.c_int32 * MAX_JOBS), ("stats", _Stats),
+                ("device_seconds", ctypes.c_double)]
+
+
+class _Work(ctypes.Structure):
+    _fields_ = [("device_seconds", ctypes.c_double), ("n_jobs", ctypes.c_int32), ("n_machines", ctypes.c_int32),
+                ("machine_pairs", ctypes.c_int32), ("explorers", ctypes.c_int32), ("warps", ctypes.c_int32),
+                ("pad", ctypes.c_int32), ("decomposed", ctypes.c_uint64), ("simple_bounds", ctypes.c_uint64),
+                ("johnson_bounds", ctypes.c_uint64), ("johnson_sweeps", ctypes.c_uint64),
+                ("sweep_free_jobs", ctypes.c_uint64), ("sweep_children", ctypes.c_uint64)]
+
+
+_lib = None
+
+
+def lib():
+    """Load libpbbperm.so (raises if it was not built)."""
+    global _lib
+    if _lib is None:
+        if not os.path.exists(LIB_PATH):
+            raise ImportError("libpbbperm.so not built: run `python -m pbbperm_b200.build`")
+        L = ctypes.CDLL(LIB_PATH)
+        L.pbb_last_error.restype = ctypes.c_char_p
+        L.pbb_config_default.argtypes = [ctypes.POINTER(_Config)]
+        L.pbb_engine_create.argtypes = [ctypes.POINTER(_Instance), ctypes.POINTER(_Config),
+                                        ctypes.POINTER(ctypes.c_void_p)]
+        L.pbb_engine_destroy.argtypes = [ctypes.c_void_p]
+        L.pbb_solve.argtypes = [ctypes.c_void_p, ctypes.c_int32, _i32p, ctypes.c_double, ctypes.POINTER(_Result)]
+        L.pbb_start.argtypes = [ctypes.c_void_p, ctypes.c_int32, _i32p]
+        L.pbb_explore.argtypes = [ctypes.c_void_p, ctypes.c_double, ctypes.POINTER(ctypes.c_int32)]
+        L.pbb_get_result.argtypes = [ctypes.c_void_p, ctypes.POINTER(_Result)]
+        L.pbb_bound_children.argtypes = [ctypes.POINTER(_Instance), ctypes.c_int32, ctypes.c_int32, ctypes.c_int32,
+                                         _i32p, _i32p, _i32p, _i32p, _i32p, _i32p, _i32p, _i32p, _i32p]
+        L.pbb_neh.argtypes = [ctypes.POINTER(_Instance), _i32p, _i32p]
+        L.pbb_start_interval.argtypes = [ctypes.c_void_p, ctypes.c_int32, _i32p, _i32p, _i32p]
+        L.pbb_set_ub.argtypes = [ctypes.c_void_p, ctypes.c_int32]
+        L.pbb_work_counters.argtypes = [ctypes.c_void_p, ctypes.POINTER(_Work)]
+        L.pbb_diag_int32_peak.argtypes = [ctypes.c_int32, ctypes.POINTER(ctypes.c_double),
+                                          ctypes.POINTER(ctypes.c_double)]
+        _lib = L
+    return _lib
+
+
+def _check(rc):
+    if rc != PBB_OK:
+        raise PbbError(rc, lib().pbb_last_error().decode())
+
+
+def _ptr(a):
+    return a.ctypes.data_as(_i32p) if a is not None else None
+
+
+def _instance(p):
+    p = np.ascontiguousarray(p, dtype=np.int32)
+    if p.ndim != 2:
+        raise ValueError("p must be a (machines x jobs) matrix")
+    inst = _Instance(p.shape[1], p.shape[0], _ptr(p))
+    return inst, p
+
+
+class Config:
+    """Search settings, named after the reference ini keys."""
+
+    def __init__(self, boundingMode=2, adaptiveBranchingMode=3, findAll=False, JohnsonMode=0,
+                 earlyStopJohnson=False, sortedDFS=0, nbIVMs=16384, device=0, warps_per_cta=0, ctas=0):
+        self.boundingMode = boundingMode
+        self.adaptiveBranchingMode = adaptiveBranchingMode
+        self.findAll = findAll
+        self.JohnsonMode = JohnsonMode
+        self.earlyStopJohnson = earlyStopJohnson
+        self.sortedDFS = sortedDFS
+        self.nbIVMs = nbIVMs
+        self.device = device
+        self.warps_per_cta = warps_per_cta
+        self.ctas = ctas
+
+    def _c(self):
+        return _Config(self.boundingMode, self.adaptiveBranchingMode, 1 if self.findAll else 0, self.JohnsonMode,
+                       1 if self.earlyStopJohnson else 0, self.sortedDFS, self.nbIVMs, self.device,
+                       self.warps_per_cta, self.ctas)
+
+
+def _result(r):
+    n = r.n_jobs
+    return dict(complete=bool(r.complete), found=bool(r.found), cost=r.cost,
+                perm=np.array(r.perm[:n], dtype=np.int32),
+                decomposed=r.stats.decomposed, johnson_bounds=r.stats.johnson_bounds,
+                simple_bounds=r.stats.simple_bounds, leaves=r.stats.leaves, steals=r.stats.steals,
+                device_seconds=r.device_seconds)
+
+
+class Engine:
+    """One instance resident on one GPU (gpubb, gpu/include/gpubb.h:101-250)."""
+
+    def __init__(self, p, config=None):
+        self.config = config or Config()
+        inst, self._p = _instance(p)
+        self.m, self.n = self._p.shape
+        h = ctypes.c_void_p()
+        cfg = self.config._c()
+        _check(lib().pbb_engine_create(ctypes.byref(inst), ctypes.byref(cfg), ctypes.byref(h)))
+        self._h = h
+
+    def close(self):
+        if getattr(self, "_h", None):
+            lib().pbb_engine_destroy(self._h)
+            self._h = None
+
+    def __del__(self):
+        self.close()
+
+    def __enter__(self):
+        return self
+
+    def __exit__(self, *a):
+        self.close()
+
+    def solve(self, ub=INF, root=None, time_limit=0.0):
+        r = _Result()
+        root = None if root is None else np.ascontiguousarray(root, dtype=np.int32)
+        _check(lib().pbb_solve(self._h, int(ub), _ptr(root), float(time_limit), ctypes.byref(r)))
+        return _result(r)
+
+    def start(self, ub=INF, root=None):
+        root = None if root is None else np.ascontiguousarray(root, dtype=np.int32)
+        _check(lib().pbb_start(self._h, int(ub), _ptr(root)))
+
+    def start_interval(self, ub, pos, end, root=None):
+        """Start on the factoradic interval [pos, end] (gpubb::initAtInterval)."""
+        root = None if root is None else np.ascontiguousarray(root, dtype=np.int32)
+        pos = np.ascontiguousarray(pos, dtype=np.int32)
+        end = np.ascontiguousarray(end, dtype=np.int32)
+        _check(lib().pbb_start_interval(self._h, int(ub), _ptr(root), _ptr(pos), _ptr(end)))
+
+    def set_ub(self, ub):
+        """Lower the incumbent to a bound found elsewhere (no permutation)."""
+        _check(lib().pbb_set_ub(self._h, int(ub)))
+
+    def kernel_stats(self):
+        """Work of the explorer kernels since start, with the INT32 op model
+        of the bounds: weak child 5m ops (add/max chain per machine); per
+        Johnson sweep and machine pair, 2 membership tests per position and
+        pass, 5 ops per free job and pass, 9 ops per evaluated child."""
+        w = _Work()
+        _check(lib().pbb_work_counters(self._h, ctypes.byref(w)))
+        m, n, P = w.n_machines, w.n_jobs, w.machine_pairs
+        ops = (5 * m * w.simple_bounds +
+               P * (4 * n * w.johnson_sweeps + 10 * w.sweep_free_jobs + 9 * w.sweep_children))
+        return dict(device_seconds=w.device_seconds, int32_ops=float(ops), decomposed=w.decomposed,
+                    simple_bounds=w.simple_bounds, johnson_bounds=w.johnson_bounds,
+                    johnson_sweeps=w.johnson_sweeps, sweep_free_jobs=w.sweep_free_jobs,
+                    sweep_children=w.sweep_children, explorers=w.explorers, warps=w.warps,
+                    work_model="5m per weak child + P*(4n per sweep + 10 per free job + 9 per child)")
+
+    def explore(self, seconds):
+        done = ctypes.c_int32(0)
+        _check(lib().pbb_explore(self._h, float(seconds), ctypes.byref(done)))
+        return bool(done.value)
+
+    def result(self):
+        r = _Result()
+        _check(lib().pbb_get_result(self._h, ctypes.byref(r)))
+        return _result(r)
+
+
+def bound_children(p, sched, limit1, limit2, johnson_mode=0, device=0):
+    """Children LBs of a batch of nodes on the GPU.
+
+    Returns dict of (count x n) arrays weak_begin, weak_end, strong_begin,
+    strong_end (by job id, 0 for fixed jobs) and (count,) node_weak,
+    node_strong."""
+    inst, p = _instance(p)
+    n = p.shape[1]
+    sched = np.ascontiguousarray(sched, dtype=np.int32).reshape(-1, n)
+    cnt = sched.shape[0]
+    l1 = np.ascontiguousarray(limit1, dtype=np.int32).reshape(cnt)
+    l2 = np.ascontiguousarray(limit2, dtype=np.int32).reshape(cnt)
+    out = {k: np.zeros((cnt, n), np.int32) for k in ("weak_begin", "weak_end", "strong_begin", "strong_end")}
+    out["node_weak"] = np.zeros(cnt, np.int32)
+    out["node_strong"] = np.zeros(cnt, np.int32)
+    _check(lib().pbb_bound_children(ctypes.byref(inst), johnson_mode, device, cnt, _ptr(sched), _ptr(l1), _ptr(l2),
+                                    _ptr(out["weak_begin"]), _ptr(out["weak_end"]), _ptr(out["strong_begin"]),
+                                    _ptr(out["strong_end"]), _ptr(out["node_weak"]), _ptr(out["node_strong"])))
+    return out
+
+
+def int32_peak(device=0):
+    """Measured INT32 add+max throughput of the GPU in Gop/s."""
+    g = ctypes.c_double(0.0)
+    t = ctypes.c_double(0.0)
+    _check(lib().pbb_diag_int32_peak(device, ctypes.byref(g), ctypes.byref(t)))
+    return g.value
+
+
+def neh(p):
+    """NEH upper bound (host code): (cost, permutation)."""
+    inst, p = _instance(p)
+    perm = np.zeros(p.shape[1], np.int32)
+    cost = np.zeros(1, np.int32)
+    _check(lib().pbb_neh(ctypes.byref(inst), _ptr(perm), _ptr(cost)))
+    return int(cost[0]), perm

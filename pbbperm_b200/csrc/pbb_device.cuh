@@ -1,0 +1,596 @@
+// Warp-level device routines of the IVM flow-shop engine (sm_100a).
+//
+// One warp owns one IVM step at a time.  Per-level vectors (pos, end, dir,
+// path job) and the current matrix row live in registers, element e of a
+// vector at lane (e % 32), word (e / 32); the instance tables live in shared
+// memory; the IVM matrix lives in HBM.  Everything is int32 and bit-exact
+// with the reference bounds (bounds/src/bound_fsp_weak.cpp,
+// bounds/src/bound_fsp_strong.cpp) and IVM navigation (multicore/src/ivm.cpp,
+// ivm_bound.cpp, sequentialbb.cpp).
+#pragma once
+#include <cuda_runtime.h>
+#include <stdint.h>
+#include "pbb_types.h"
+
+#define FULLMASK 0xffffffffu
+#define NEG_INF (-(1 << 28))
+
+namespace pbb {
+
+__device__ __forceinline__ int lane_id() { return threadIdx.x & 31; }
+__device__ __forceinline__ unsigned lanemask_lt() { return (1u << lane_id()) - 1u; }
+
+// job stored in a cell, whatever its pruning flag (common/include/misc.h absolute())
+__device__ __forceinline__ int cell_job(int v) { return v >= 0 ? v : -v - 1; }
+// flagged form of a cell (misc.h negative())
+__device__ __forceinline__ int cell_flag(int v) { return v < 0 ? v : -v - 1; }
+
+// element `idx` (warp-uniform) of a lane-distributed vector
+template <int NW>
+__device__ __forceinline__ int vget(const int (&x)[NW], int idx)
+{
+    int src = x[0];
+#pragma unroll
+    for (int w = 1; w < NW; w++)
+        if ((idx >> 5) == w) src = x[w];
+    return __shfl_sync(FULLMASK, src, idx & 31);
+}
+
+// element `s` (per lane) of a lane-distributed vector
+template <int NW>
+__device__ __forceinline__ int vgather(const int (&x)[NW], int s)
+{
+    int r = 0;
+#pragma unroll
+    for (int w = 0; w < NW; w++) {
+        int t = __shfl_sync(FULLMASK, x[w], s & 31);
+        if ((s >> 5) == w) r = t;
+    }
+    return r;
+}
+
+template <int NW>
+__device__ __forceinline__ void vset(int (&x)[NW], int idx, int val)
+{
+    if (lane_id() == (idx & 31)) {
+#pragma unroll
+        for (int w = 0; w < NW; w++)
+            if ((idx >> 5) == w) x[w] = val;
+    }
+}
+
+// ivm.cpp:194-202 -- lexicographic pos <= end over the n levels
+template <int NW>
+__device__ __forceinline__ bool before_end(const int (&pos)[NW], const int (&end)[NW], int n)
+{
+#pragma unroll
+    for (int w = 0; w < NW; w++) {
+        int lv = w * 32 + lane_id();
+        unsigned d = __ballot_sync(FULLMASK, lv < n && pos[w] != end[w]);
+        if (d) {
+            int f = __ffs(d) - 1;
+            int pp = __shfl_sync(FULLMASK, pos[w], f);
+            int ee = __shfl_sync(FULLMASK, end[w], f);
+            return pp < ee;
+        }
+    }
+    return true;
+}
+
+// first unpruned cell of the row at index >= from (and < k), or k
+template <int NW>
+__device__ __forceinline__ int next_open_cell(const int (&row)[NW], int from, int k)
+{
+#pragma unroll
+    for (int w = 0; w < NW; w++) {
+        int idx = w * 32 + lane_id();
+        unsigned b = __ballot_sync(FULLMASK, idx >= from && idx < k && row[w] >= 0);
+        if (b) return w * 32 + __ffs(b) - 1;
+    }
+    return k;
+}
+
+// ---------------------------------------------------------------------------
+// shared-memory views
+// ---------------------------------------------------------------------------
+struct CtaTables {
+    const unsigned long long* je;  // [n][Ppad]
+    const int* p;                  // [m][n]
+    const unsigned char* pm0;
+    const unsigned char* pm1;
+    const int* min_arr;
+    const int* min_dep;
+    int n, m, P, Ppad;
+};
+
+struct WarpScratch {
+    int* lbF;     // [64] Johnson LB of front children, by job
+    int* lbB;     // [64]
+    int* frontZ;  // [32] heads of the front jobs (zero based)
+    int* backZ;   // [32] tails of the back jobs (zero based)
+    int* Fb;      // [32] front used by the bounds (earliest starts when no front job)
+    int* Bb;      // [32] back used by the bounds (min run-outs when no back job)
+    int* rem;     // [32] machine loads of the free jobs
+    int* RB;      // [32] rem + Bb
+    int* FR;      // [32] Fb + rem
+    short* dF;    // [64][m] heads of front child u minus frontZ
+    short* dB;    // [64][m] tails of back child u minus backZ
+    unsigned char* fjob;  // [64] front jobs in schedule order
+    unsigned char* bjob;  // [64] back jobs, last position first
+    unsigned char* rowj;  // [64] free jobs (row order)
+};
+
+__device__ __forceinline__ WarpScratch warp_scratch(unsigned char* base, int m)
+{
+    WarpScratch s;
+    int* ip = reinterpret_cast<int*>(base);
+    s.lbF = ip; ip += PBB_MAX_N;
+    s.lbB = ip; ip += PBB_MAX_N;
+    s.frontZ = ip; ip += 32;
+    s.backZ = ip; ip += 32;
+    s.Fb = ip; ip += 32;
+    s.Bb = ip; ip += 32;
+    s.rem = ip; ip += 32;
+    s.RB = ip; ip += 32;
+    s.FR = ip; ip += 32;
+    short* sp = reinterpret_cast<short*>(ip);
+    s.dF = sp; sp += PBB_MAX_N * m;
+    s.dB = sp; sp += PBB_MAX_N * m;
+    unsigned char* bp = reinterpret_cast<unsigned char*>(sp);
+    s.fjob = bp; bp += PBB_MAX_N;
+    s.bjob = bp; bp += PBB_MAX_N;
+    s.rowj = bp;
+    return s;
+}
+
+// ---------------------------------------------------------------------------
+// partial schedules
+// ---------------------------------------------------------------------------
+
+// Heads of fjob[0..f) and tails of bjob[0..b), both from zero, one machine per
+// lane, as a diagonal wavefront (bound_fsp_weak.cpp:62-107 restated).  Then
+// the bound-side front/back: earliest starts when nothing is fixed in front,
+// minimum run-outs when nothing is fixed at the back (:62-66, :86-90), and the
+// loads of the free jobs (:110-122).
+__device__ __forceinline__ void partial_schedule(const CtaTables& T, const WarpScratch& S, int f, int b, int k)
+{
+    const int lane = lane_id();
+    const int n = T.n, m = T.m;
+    int cf = 0, cb = 0;
+    const int steps = (f > b ? f : b) + m - 1;
+    const int ib0 = m - 1 - lane;
+    for (int s = 0; s < steps; s++) {
+        int upf = __shfl_up_sync(FULLMASK, cf, 1);
+        int dnb = __shfl_down_sync(FULLMASK, cb, 1);
+        if (lane == 0) upf = 0;
+        if (lane == m - 1) dnb = 0;
+        int i = s - lane;
+        if (lane < m && i >= 0 && i < f) cf = max(cf, upf) + T.p[lane * n + S.fjob[i]];
+        int ib = s - ib0;
+        if (lane < m && ib >= 0 && ib < b) cb = max(cb, dnb) + T.p[lane * n + S.bjob[ib]];
+    }
+    if (lane < m) {
+        // loads of the free jobs: sum the shorter of the free / fixed lists
+        int r = 0;
+        if (k <= n - k) {
+            for (int i = 0; i < k; i++) r += T.p[lane * n + S.rowj[i]];
+        } else {
+            for (int j = 0; j < n; j++) r += T.p[lane * n + j];
+            for (int i = 0; i < f; i++) r -= T.p[lane * n + S.fjob[i]];
+            for (int i = 0; i < b; i++) r -= T.p[lane * n + S.bjob[i]];
+        }
+        int fb = (f == 0) ? T.min_arr[lane] : cf;
+        int bb = (b == 0) ? T.min_dep[lane] : cb;
+        S.frontZ[lane] = cf;
+        S.backZ[lane] = cb;
+        S.Fb[lane] = fb;
+        S.Bb[lane] = bb;
+        S.rem[lane] = r;
+        S.RB[lane] = r + bb;
+        S.FR[lane] = fb + r;
+    }
+    __syncwarp();
+}
+
+// weak node LB (bound_fsp_weak.cpp:289-311), read by every lane
+__device__ __forceinline__ int weak_node_lb(const CtaTables& T, const WarpScratch& S)
+{
+    int t0 = S.Fb[0] + S.rem[0];
+    int lb = t0 + S.Bb[0];
+    for (int k = 1; k < T.m; k++) {
+        int t1 = max(S.FR[k], t0);
+        lb = max(lb, t1 + S.Bb[k]);
+        t0 = t1;
+    }
+    return lb;
+}
+
+// weak LB of child u appended at the front (bound_fsp_weak.cpp:134-161)
+__device__ __forceinline__ int weak_front(const CtaTables& T, const WarpScratch& S, int u)
+{
+    const int n = T.n;
+    int t0 = S.Fb[0] + T.p[u];
+    int lb = S.Fb[0] + S.RB[0];
+    for (int k = 1; k < T.m; k++) {
+        int t1 = max(S.Fb[k], t0);
+        lb = max(lb, t1 + S.RB[k]);
+        t0 = t1 + T.p[k * n + u];
+    }
+    return lb;
+}
+
+// weak LB of child u prepended at the back (bound_fsp_weak.cpp:164-191)
+__device__ __forceinline__ int weak_back(const CtaTables& T, const WarpScratch& S, int u)
+{
+    const int n = T.n, m = T.m;
+    int t0 = S.Bb[m - 1] + T.p[(m - 1) * n + u];
+    int lb = S.FR[m - 1] + S.Bb[m - 1];
+    for (int k = m - 2; k >= 0; k--) {
+        int t1 = max(t0, S.Bb[k]);
+        lb = max(lb, S.FR[k] + t1);
+        t0 = t1 + T.p[k * n + u];
+    }
+    return lb;
+}
+
+// makespan of  front jobs + x + y + back jobs  (y < 0: front + x + back),
+// as max over machines of head + tail at the split
+__device__ __forceinline__ int makespan_split(const CtaTables& T, const WarpScratch& S, int x, int y)
+{
+    const int n = T.n;
+    int h1 = 0, h2 = 0, best = 0;
+    for (int k = 0; k < T.m; k++) {
+        h1 = max(h1, S.frontZ[k]) + T.p[k * n + x];
+        int h = h1;
+        if (y >= 0) { h2 = max(h2, h1) + T.p[k * n + y]; h = h2; }
+        best = max(best, h + S.backZ[k]);
+    }
+    return best;
+}
+
+// ---------------------------------------------------------------------------
+// Johnson two-machine bound of children (bound_fsp_strong.cpp:103-162 per child)
+// ---------------------------------------------------------------------------
+//
+// For machine pair (a, b) with lag c and the free jobs U in Johnson order,
+// the reference scans  t0 += a_j ; t1 = max(t1, t0 + c_j) + b_j  from
+// (t0, t1) = (front[a], front[b]) and closes with max(t1 + back[b], t0 + back[a]).
+// This map is max-plus linear: over a sequence it equals
+//   t0' = t0 + A,   t1' = max(t1 + B, t0 + C),   C = max_s (Apre_s + c_s + Bsuf_s).
+// Dropping the child's own job q from U gives
+//   C_{-q} = max( max_{s<q} W_s - b_q , max_{s>q} W_s - a_q ),  W_s = Apre_s + c_s + Bsuf_s
+// so one forward and one backward sweep per pair yield the LB of every child
+// at once, exactly (integer max/+ only).  Lanes own machine pairs; the
+// per-child maxima are merged with shared-memory atomicMax by job id.
+//
+// doF / doB select front / back children; sF / sB are job masks of the
+// children to evaluate.  Results land in S.lbF / S.lbB (0 = not evaluated).
+template <int NW>
+__device__ __forceinline__ void johnson_children(const CtaTables& T, const WarpScratch& S,
+                                                 const unsigned (&um)[NW], bool doF, const unsigned (&sF)[NW],
+                                                 bool doB, const unsigned (&sB)[NW], int* node_lb)
+{
+    const int lane = lane_id();
+    const int n = T.n, m = T.m;
+    int nodeAcc = 0;
+    for (int base = 0; base < T.P; base += 32) {
+        const int i = base + lane;
+        const bool act = i < T.P;
+        const int m0 = act ? T.pm0[i] : 0;
+        const int m1 = act ? T.pm1[i] : 0;
+        const int Asum = S.rem[m0], Bsum = S.rem[m1];
+        // front children: F = frontZ + dF[u], B = Bb
+        const int cF1 = S.frontZ[m1] + Bsum + S.Bb[m1];
+        const int cF2 = S.frontZ[m0] + S.Bb[m1];
+        const int cF3 = S.frontZ[m0] + Asum + S.Bb[m0];
+        // back children: F = Fb, B = backZ + dB[u]
+        const int cB1 = S.Fb[m1] + Bsum + S.backZ[m1];
+        const int cB2 = S.Fb[m0] + S.backZ[m1];
+        const int cB3 = S.Fb[m0] + Asum + S.backZ[m0];
+        const unsigned long long* col = T.je + i;
+        int Apre = 0, Bpre = 0, PMx = NEG_INF;
+        if (act) {
+            for (int t = 0; t < n; t++) {
+                const unsigned long long e = col[t * T.Ppad];
+                const int u = JE_JOB(e);
+                const unsigned bit = 1u << (u & 31);
+                unsigned uw = um[0], fw = sF[0], bw = sB[0];
+#pragma unroll
+                for (int w = 1; w < NW; w++)
+                    if ((u >> 5) == w) { uw = um[w]; fw = sF[w]; bw = sB[w]; }
+                if (uw & bit) {
+                    const int a = JE_A(e), b = JE_B(e), c = JE_C(e);
+                    Apre += a;
+                    const int W = Apre - Bpre + c + Bsum;
+                    if (doF && (fw & bit)) {
+                        const int d0 = S.dF[u * m + m0], d1 = S.dF[u * m + m1];
+                        int v = max(cF1 + d1 - b, cF2 + d0 + PMx - b);
+                        v = max(v, cF3 + d0 - a);
+                        atomicMax(&S.lbF[u], v);
+                    }
+                    if (doB && (bw & bit)) {
+                        const int d0 = S.dB[u * m + m0], d1 = S.dB[u * m + m1];
+                        int v = max(cB1 - b, cB2 + PMx - b) + d1;
+                        v = max(v, cB3 - a + d0);
+                        atomicMax(&S.lbB[u], v);
+                    }
+                    PMx = max(PMx, W);
+                    Bpre += b;
+                }
+            }
+            if (node_lb) {
+                // the node itself (nothing removed): bornes_calculer of the node
+                int v = max(S.Fb[m1] + Bsum + S.Bb[m1], S.Fb[m0] + PMx + S.Bb[m1]);
+                v = max(v, S.Fb[m0] + Asum + S.Bb[m0]);
+                nodeAcc = max(nodeAcc, v);
+            }
+            int Asuf = 0, Bsuf = 0, SMx = NEG_INF;
+            for (int t = n - 1; t >= 0; t--) {
+                const unsigned long long e = col[t * T.Ppad];
+                const int u = JE_JOB(e);
+                const unsigned bit = 1u << (u & 31);
+                unsigned uw = um[0], fw = sF[0], bw = sB[0];
+#pragma unroll
+                for (int w = 1; w < NW; w++)
+                    if ((u >> 5) == w) { uw = um[w]; fw = sF[w]; bw = sB[w]; }
+                if (uw & bit) {
+                    const int a = JE_A(e), b = JE_B(e), c = JE_C(e);
+                    if (doF && (fw & bit)) {
+                        const int d0 = S.dF[u * m + m0];
+                        atomicMax(&S.lbF[u], cF2 + d0 + SMx - a);
+                    }
+                    if (doB && (bw & bit)) {
+                        const int d1 = S.dB[u * m + m1];
+                        atomicMax(&S.lbB[u], cB2 + SMx - a + d1);
+                    }
+                    Bsuf += b;
+                    SMx = max(SMx, Asum - Asuf + c + Bsuf);
+                    Asuf += a;
+                }
+            }
+        }
+    }
+    if (node_lb) {
+        for (int o = 16; o; o >>= 1) nodeAcc = max(nodeAcc, __shfl_xor_sync(FULLMASK, nodeAcc, o));
+        *node_lb = nodeAcc;
+    }
+    __syncwarp();
+}
+
+// Per-child head/tail deltas used by johnson_children (front child u: heads of
+// front + u; back child u: tails of u + back).  Lane per free cell.
+template <int NW>
+__device__ __forceinline__ void child_tables(const CtaTables& T, const WarpScratch& S, const int (&row)[NW], int k,
+                                             bool doF, const unsigned (&sF)[NW], bool doB, const unsigned (&sB)[NW])
+{
+    const int n = T.n, m = T.m;
+#pragma unroll
+    for (int w = 0; w < NW; w++) {
+        const int idx = w * 32 + lane_id();
+        if (idx < k) {
+            const int u = row[w];
+            const unsigned bit = 1u << (u & 31);
+            unsigned fw = sF[0], bw = sB[0];
+#pragma unroll
+            for (int q = 1; q < NW; q++)
+                if ((u >> 5) == q) { fw = sF[q]; bw = sB[q]; }
+            if (doF && (fw & bit)) {
+                int h = 0;
+                for (int kk = 0; kk < m; kk++) {
+                    const int z = S.frontZ[kk];
+                    h = max(h, z) + T.p[kk * n + u];
+                    S.dF[u * m + kk] = (short)(h - z);
+                }
+            }
+            if (doB && (bw & bit)) {
+                int t = 0;
+                for (int kk = m - 1; kk >= 0; kk--) {
+                    const int z = S.backZ[kk];
+                    t = max(t, z) + T.p[kk * n + u];
+                    S.dB[u * m + kk] = (short)(t - z);
+                }
+            }
+        }
+    }
+    __syncwarp();
+}
+
+// job bitmask of the lanes' cells where pred holds
+template <int NW>
+__device__ __forceinline__ void job_mask(unsigned (&out)[NW], const int (&row)[NW], const bool (&pred)[NW])
+{
+#pragma unroll
+    for (int q = 0; q < NW; q++) {
+        unsigned v = 0;
+#pragma unroll
+        for (int w = 0; w < NW; w++)
+            if (pred[w] && ((row[w] >> 5) == q)) v |= 1u << (row[w] & 31);
+        out[q] = __reduce_or_sync(FULLMASK, v);
+    }
+}
+
+// Branching rule (ivm_bound.cpp:413-560, CPU numbering), evaluated over the
+// free children only: fixed jobs have cost 0 on both sides and contribute
+// nothing to any rule.  Returns 0 = FRONT, 1 = BACK.
+template <int NW>
+__device__ __forceinline__ int choose_dir(int rule, int line, int ub, const int (&cb)[NW], const int (&ce)[NW],
+                                          const bool (&valid)[NW])
+{
+    switch (rule) {
+    case -3: return (line & 1) ? 1 : 0;
+    case -2: return 1;
+    case -1: return 0;
+    case 1: {
+        int s = 0;
+#pragma unroll
+        for (int w = 0; w < NW; w++) if (valid[w]) s += cb[w] - ce[w];
+        s = __reduce_add_sync(FULLMASK, s);
+        return s < 0 ? 1 : 0;
+    }
+    case 2: {
+        int elim = 0, s = 0;
+#pragma unroll
+        for (int w = 0; w < NW; w++) {
+            if (!valid[w]) continue;
+            if (cb[w] >= ub) elim++; else s += cb[w];
+            if (ce[w] >= ub) elim--; else s -= ce[w];
+        }
+        elim = __reduce_add_sync(FULLMASK, elim);
+        s = __reduce_add_sync(FULLMASK, s);
+        if (elim > 0) return 0;
+        if (elim < 0) return 1;
+        return s < 0 ? 1 : 0;
+    }
+    default: {   // 3: MinMin, ties broken by the eliminated count
+        unsigned mn = 0x7fffffffu;
+#pragma unroll
+        for (int w = 0; w < NW; w++) {
+            if (!valid[w]) continue;
+            if (cb[w] > 0) mn = min(mn, (unsigned)cb[w]);
+            if (ce[w] > 0) mn = min(mn, (unsigned)ce[w]);
+        }
+        mn = __reduce_min_sync(FULLMASK, mn);
+        int cnt = 0, elim = 0;
+#pragma unroll
+        for (int w = 0; w < NW; w++) {
+            if (!valid[w]) continue;
+            if ((unsigned)cb[w] == mn) cnt++;
+            if ((unsigned)ce[w] == mn) cnt--;
+            if (cb[w] >= ub) elim++;
+            if (ce[w] >= ub) elim--;
+        }
+        cnt = __reduce_add_sync(FULLMASK, cnt);
+        elim = __reduce_add_sync(FULLMASK, elim);
+        if (cnt > 0) return 1;
+        if (cnt < 0) return 0;
+        return elim > 0 ? 0 : 1;
+    }
+    }
+}
+
+struct NodeCounters {
+    unsigned long long simple, johnson;
+    unsigned long long sweeps, free_jobs, swept_children;
+};
+
+// Bound the children of the node whose free jobs are `row[0..k)` (front and
+// back lists already in S.fjob / S.bjob, f and b long), choose the branching
+// side and prune the row in place (ivm_bound.cpp weak/strong/mixedBoundPrune
+// :650-676 -> chooseChildrenSet, prune :611-646 with sortedDFS = 0).
+// Returns the side chosen for this level.
+template <int NW>
+__device__ __forceinline__ int bound_and_prune(const CtaTables& T, const WarpScratch& S, const DevSearch& srch,
+                                               int mode, int (&row)[NW], int k, int f, int b, int line,
+                                               int prev_dir, int best, NodeCounters& cnt)
+{
+    const int lane = lane_id();
+    bool valid[NW];
+#pragma unroll
+    for (int w = 0; w < NW; w++) valid[w] = (w * 32 + lane) < k;
+#pragma unroll
+    for (int w = 0; w < NW; w++)
+        if (valid[w]) S.rowj[w * 32 + lane] = (unsigned char)row[w];
+    __syncwarp();
+    partial_schedule(T, S, f, b, k);
+
+    const bool both = srch.branch_mode > 0;
+    const bool fa = srch.find_all != 0;
+    int cbw[NW], cew[NW], cbs[NW], ces[NW];
+#pragma unroll
+    for (int w = 0; w < NW; w++) { cbw[w] = 0; cew[w] = 0; cbs[w] = 0; ces[w] = 0; }
+
+    int dir;
+    if (mode != 1) {
+#pragma unroll
+        for (int w = 0; w < NW; w++) {
+            if (valid[w]) {
+                cbw[w] = weak_front(T, S, row[w]);
+                if (both) cew[w] = weak_back(T, S, row[w]);
+            }
+        }
+        cnt.simple += both ? 2 * k : k;
+        dir = choose_dir<NW>(srch.branch_mode, line, best, cbw, cew, valid);
+    }
+
+    if (mode != 0) {
+        bool doF = (mode == 1) || dir == 0;
+        bool doB = (mode == 1) || dir == 1;
+        bool pF[NW], pB[NW];
+#pragma unroll
+        for (int w = 0; w < NW; w++) {
+            // mode 2 evaluates only the children the weak bound keeps (ivm_bound.cpp:168)
+            bool keepF = (mode == 1) || !(fa ? cbw[w] > best : cbw[w] >= best);
+            bool keepB = (mode == 1) || !(fa ? cew[w] > best : cew[w] >= best);
+            pF[w] = valid[w] && doF && keepF;
+            pB[w] = valid[w] && doB && keepB;
+        }
+        unsigned sF[NW], sB[NW], um[NW];
+        job_mask<NW>(sF, row, pF);
+        job_mask<NW>(sB, row, pB);
+        job_mask<NW>(um, row, valid);
+        int nF = 0, nB = 0;
+#pragma unroll
+        for (int q = 0; q < NW; q++) { nF += __popc(sF[q]); nB += __popc(sB[q]); }
+        cnt.johnson += nF + nB;
+        if (nF + nB > 0) {
+            if (k <= 2) {
+                // each child has at most one free job left: exact makespan
+                // (bound_fsp_strong.cpp:543-546)
+                const int x = vget<NW>(row, 0);
+                const int y = k == 2 ? vget<NW>(row, 1) : -1;
+                int mk = 0;
+                if (lane < 2) mk = makespan_split(T, S, lane == 0 ? x : y, lane == 0 ? y : x);
+                const int mxy = __shfl_sync(FULLMASK, mk, 0);
+                const int myx = __shfl_sync(FULLMASK, mk, 1);
+#pragma unroll
+                for (int w = 0; w < NW; w++) {
+                    if (pF[w]) cbs[w] = (row[w] == x) ? mxy : myx;
+                    if (pB[w]) ces[w] = (row[w] == x) ? myx : mxy;
+                }
+            } else {
+#pragma unroll
+                for (int w = 0; w < NW; w++) {
+                    if (w * 32 + lane < PBB_MAX_N) { S.lbF[w * 32 + lane] = 0; S.lbB[w * 32 + lane] = 0; }
+                }
+                child_tables<NW>(T, S, row, k, nF > 0, sF, nB > 0, sB);
+                johnson_children<NW>(T, S, um, nF > 0, sF, nB > 0, sB, nullptr);
+                cnt.sweeps++;
+                cnt.free_jobs += k;
+                cnt.swept_children += nF + nB;
+#pragma unroll
+                for (int w = 0; w < NW; w++) {
+                    if (pF[w]) cbs[w] = S.lbF[row[w]];
+                    if (pB[w]) ces[w] = S.lbB[row[w]];
+                }
+            }
+        }
+        if (mode == 1) dir = choose_dir<NW>(srch.branch_mode, line, best, cbs, ces, valid);
+    }
+
+    // prune: mark children whose bound reaches the incumbent (eliminateJobs :338-410)
+#pragma unroll
+    for (int w = 0; w < NW; w++) {
+        int c1, c2;
+        if (mode == 1) { c1 = dir ? ces[w] : cbs[w]; c2 = c1; }
+        else if (mode == 0) { c1 = dir ? cew[w] : cbw[w]; c2 = c1; }
+        else { c1 = dir ? cew[w] : cbw[w]; c2 = dir ? ces[w] : cbs[w]; }
+        bool cut = fa ? (c1 > best || c2 > best) : (c1 >= best || c2 >= best);
+        if (valid[w] && cut) row[w] = cell_flag(row[w]);
+    }
+    // reverse the row when the side changes from the previous level (:620-636)
+    if (prev_dir != dir) {
+        int nr[NW];
+#pragma unroll
+        for (int w = 0; w < NW; w++) {
+            int idx = w * 32 + lane;
+            int src = k - 1 - idx;
+            int v = vgather<NW>(row, src < 0 ? 0 : src);
+            nr[w] = (idx < k) ? v : row[w];
+        }
+#pragma unroll
+        for (int w = 0; w < NW; w++) row[w] = nr[w];
+    }
+    return dir;
+}
+
+}  // namespace pbb

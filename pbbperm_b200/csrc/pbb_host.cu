@@ -1,0 +1,646 @@
+// Host side of the engine: instance tables, device memory, launches, and the
+// C ABI declared in include/pbbperm.h.
+#include <cuda_runtime.h>
+#include <stdint.h>
+#include <string.h>
+
+#include <algorithm>
+#include <chrono>
+#include <climits>
+#include <string>
+#include <vector>
+
+#include "pbb_types.h"
+#include "pbb_launch.h"
+#include "../../include/pbbperm.h"
+#include "../../include/pbbperm_diag.h"
+
+namespace {
+
+thread_local std::string g_err;
+
+int fail(int code, const std::string& msg)
+{
+    g_err = msg;
+    return code;
+}
+
+int cuda_fail(cudaError_t e, const char* where)
+{
+    g_err = std::string(where) + ": " + cudaGetErrorString(e);
+    return e == cudaErrorMemoryAllocation ? PBB_E_NOMEM : PBB_E_CUDA;
+}
+
+#define CK(call)                                        \
+    do {                                                \
+        cudaError_t e_ = (call);                        \
+        if (e_ != cudaSuccess) return cuda_fail(e_, #call); \
+    } while (0)
+
+// ---------------------------------------------------------------------------
+// instance tables
+// ---------------------------------------------------------------------------
+struct HostTables {
+    int n = 0, m = 0, P = 0, Ppad = 0;
+    std::vector<int> p, min_arr, min_dep;
+    std::vector<unsigned long long> je;
+    std::vector<unsigned char> pm0, pm1;
+};
+
+// Johnson's rule with the reference's tie order: keys (group, value); group 1
+// (first machine strictly shorter) ascending by p_a + lag, then group 2
+// descending by p_b + lag; equal keys stay in the order left by a Hoare
+// partition quicksort that pivots on the first element
+// (bounds/src/bound_fsp_strong.cpp:359-436).  The order among ties changes
+// the bound's value, so the partition scheme is part of the contract.
+struct JohnsonKeys {
+    std::vector<int> grp, val;
+    bool before(int x, int y) const
+    {
+        if (grp[x] != grp[y]) return grp[x] < grp[y];
+        return grp[x] == 1 ? val[x] < val[y] : val[x] > val[y];
+    }
+    bool after(int x, int y) const
+    {
+        if (grp[x] != grp[y]) return grp[x] > grp[y];
+        return grp[x] == 1 ? val[x] > val[y] : val[x] < val[y];
+    }
+};
+
+void hoare_sort(const JohnsonKeys& K, std::vector<int>& v, int lo, int hi)
+{
+    while (lo < hi) {
+        const int pivot = v[lo];
+        int i = lo - 1, j = hi + 1;
+        while (true) {
+            do { --j; } while (K.after(v[j], pivot));
+            do { ++i; } while (K.before(v[i], pivot));
+            if (i >= j) break;
+            std::swap(v[i], v[j]);
+        }
+        hoare_sort(K, v, lo, j);
+        lo = j + 1;
+    }
+}
+
+int build_tables(const pbb_instance* inst, int johnson_mode, HostTables& H)
+{
+    if (!inst || !inst->p) return fail(PBB_E_INVAL, "instance is NULL");
+    const int n = inst->n_jobs, m = inst->n_machines;
+    if (n < 2 || n > PBB_MAX_JOBS) return fail(PBB_E_INVAL, "n_jobs must be in [2, 64]");
+    if (m < 2 || m > PBB_MAX_MACHINES) return fail(PBB_E_INVAL, "n_machines must be in [2, 32]");
+    if (johnson_mode < 0 || johnson_mode > 2) return fail(PBB_E_UNSUPPORTED, "JohnsonMode must be 0, 1 or 2");
+    H.n = n; H.m = m;
+    H.p.assign(inst->p, inst->p + n * m);
+    long long total = 0;
+    for (int j = 0; j < n; j++) {
+        long long s = 0;
+        for (int k = 0; k < m; k++) {
+            const int v = H.p[k * n + j];
+            if (v < 0 || v > 65535) return fail(PBB_E_INVAL, "processing times must be in [0, 65535]");
+            s += v;
+        }
+        if (s > 32767) return fail(PBB_E_INVAL, "a job's total processing time must be <= 32767");
+        total += s;
+    }
+    if (total > (1 << 26)) return fail(PBB_E_INVAL, "instance total processing time too large");
+    // earliest start / minimum run-out per machine (bound_fsp_weak.cpp:249-286)
+    H.min_arr.assign(m, INT_MAX);
+    H.min_dep.assign(m, INT_MAX);
+    H.min_arr[0] = 0;
+    H.min_dep[m - 1] = 0;
+    for (int j = 0; j < n; j++) {
+        int head = 0;
+        for (int k = 1; k < m; k++) {
+            head += H.p[(k - 1) * n + j];
+            H.min_arr[k] = std::min(H.min_arr[k], head);
+        }
+        int tail = 0;
+        for (int k = m - 2; k >= 0; k--) {
+            tail += H.p[(k + 1) * n + j];
+            H.min_dep[k] = std::min(H.min_dep[k], tail);
+        }
+    }
+    // machine pairs in the reference's order (bound_fsp_strong.cpp:283-297),
+    // filtered by JohnsonMode (:133-135)
+    std::vector<std::pair<int, int>> pairs;
+    for (int a = 0; a < m - 1; a++)
+        for (int b = a + 1; b < m; b++) {
+            if (johnson_mode == 1 && b < m - 1) continue;
+            if (johnson_mode == 2 && b != a + 1) continue;
+            pairs.push_back({a, b});
+        }
+    H.P = (int)pairs.size();
+    H.Ppad = (H.P + 31) / 32 * 32;
+    H.je.assign((size_t)n * H.Ppad, 0ull);
+    H.pm0.assign(H.Ppad, 0);
+    H.pm1.assign(H.Ppad, 0);
+    JohnsonKeys K;
+    K.grp.resize(n);
+    K.val.resize(n);
+    std::vector<int> lag(n), order(n);
+    for (int i = 0; i < H.P; i++) {
+        const int a = pairs[i].first, b = pairs[i].second;
+        H.pm0[i] = (unsigned char)a;
+        H.pm1[i] = (unsigned char)b;
+        for (int j = 0; j < n; j++) {
+            int l = 0;
+            for (int k = a + 1; k < b; k++) l += H.p[k * n + j];
+            lag[j] = l;
+            const int pa = H.p[a * n + j], pb = H.p[b * n + j];
+            K.grp[j] = pa < pb ? 1 : 2;
+            K.val[j] = (pa < pb ? pa : pb) + l;
+            order[j] = j;
+        }
+        hoare_sort(K, order, 0, n - 1);
+        for (int t = 0; t < n; t++) {
+            const int j = order[t];
+            const unsigned long long e = (unsigned long long)j | ((unsigned long long)H.p[a * n + j] << 8) |
+                                         ((unsigned long long)H.p[b * n + j] << 24) |
+                                         ((unsigned long long)lag[j] << 40);
+            H.je[(size_t)t * H.Ppad + i] = e;
+        }
+    }
+    return PBB_OK;
+}
+
+struct DeviceInstance {
+    int* p = nullptr;
+    unsigned long long* je = nullptr;
+    unsigned char* pm = nullptr;
+    int* mt = nullptr;
+    DevInstance view{};
+
+    int upload(const HostTables& H, cudaStream_t st)
+    {
+        CK(cudaMalloc(&p, sizeof(int) * H.n * H.m));
+        CK(cudaMalloc(&je, sizeof(unsigned long long) * H.je.size()));
+        CK(cudaMalloc(&pm, 2 * H.Ppad));
+        CK(cudaMalloc(&mt, sizeof(int) * 2 * H.m));
+        CK(cudaMemcpyAsync(p, H.p.data(), sizeof(int) * H.n * H.m, cudaMemcpyHostToDevice, st));
+        CK(cudaMemcpyAsync(je, H.je.data(), sizeof(unsigned long long) * H.je.size(), cudaMemcpyHostToDevice, st));
+        CK(cudaMemcpyAsync(pm, H.pm0.data(), H.Ppad, cudaMemcpyHostToDevice, st));
+        CK(cudaMemcpyAsync(pm + H.Ppad, H.pm1.data(), H.Ppad, cudaMemcpyHostToDevice, st));
+        CK(cudaMemcpyAsync(mt, H.min_arr.data(), sizeof(int) * H.m, cudaMemcpyHostToDevice, st));
+        CK(cudaMemcpyAsync(mt + H.m, H.min_dep.data(), sizeof(int) * H.m, cudaMemcpyHostToDevice, st));
+        view.n = H.n; view.m = H.m; view.P = H.P; view.Ppad = H.Ppad;
+        view.p = p; view.je = je; view.pm0 = pm; view.pm1 = pm + H.Ppad;
+        view.min_arr = mt; view.min_dep = mt + H.m;
+        return PBB_OK;
+    }
+    void release()
+    {
+        cudaFree(p); cudaFree(je); cudaFree(pm); cudaFree(mt);
+        p = nullptr; je = nullptr; pm = nullptr; mt = nullptr;
+    }
+};
+
+int max_smem_optin(int dev)
+{
+    int v = 0;
+    cudaDeviceGetAttribute(&v, cudaDevAttrMaxSharedMemoryPerBlockOptin, dev);
+    return v;
+}
+
+int pick_warps(const HostTables& H, int requested, int dev, int& smem)
+{
+    const int cap = max_smem_optin(dev);
+    int w = requested > 0 ? std::min(requested, PBB_WARPS_MAX) : PBB_WARPS_MAX;
+    for (; w >= 1; w--) {
+        smem = pbbl::smem_bytes(H.n, H.m, H.Ppad, w);
+        if (smem <= cap) return w;
+    }
+    return 0;
+}
+
+}  // namespace
+
+// ---------------------------------------------------------------------------
+// engine
+// ---------------------------------------------------------------------------
+struct pbb_engine {
+    pbb_config cfg{};
+    HostTables H;
+    int dev = 0;
+    cudaStream_t st = nullptr;
+    cudaEvent_t ev0 = nullptr, ev1 = nullptr;
+    int nw = 2, warps = 0, ctas = 0, smem = 0, root_smem = 0;
+    DeviceInstance di;
+    signed char *mat = nullptr, *vec = nullptr, *bestperm = nullptr;
+    int *line = nullptr, *state = nullptr, *bestcost = nullptr, *qval = nullptr, *ub_d = nullptr, *root_d = nullptr;
+    int* ival_d = nullptr;   // [2][64] interval start / end vectors
+    unsigned* qseq = nullptr;
+    GroupCtl* ctl = nullptr;
+    DevGroup* group_d = nullptr;
+    DevGroup group{};
+    double dev_seconds = 0.0;
+    bool started = false, done = false;
+    int32_t ub = INT32_MAX;
+    double slice_s = 2.0;
+    int select_budget = 4096;
+};
+
+extern "C" {
+
+void pbb_config_default(pbb_config* c)
+{
+    if (!c) return;
+    memset(c, 0, sizeof(*c));
+    c->bounding_mode = 2;
+    c->branching_mode = 3;
+    c->find_all = 0;
+    c->johnson_mode = 0;
+    c->early_stop_johnson = 0;
+    c->sorted_dfs = 0;
+    c->nb_ivms = 16384;
+    c->device = 0;
+}
+
+const char* pbb_last_error(void) { return g_err.c_str(); }
+
+static int check_config(const pbb_config* c)
+{
+    if (c->bounding_mode < 0 || c->bounding_mode > 2) return fail(PBB_E_INVAL, "boundingMode must be 0, 1 or 2");
+    const int b = c->branching_mode;
+    if (!(b == -3 || b == -2 || b == -1 || b == 1 || b == 2 || b == 3))
+        return fail(PBB_E_INVAL, "adaptiveBranchingMode must be one of -3,-2,-1,1,2,3");
+    if (c->early_stop_johnson) return fail(PBB_E_UNSUPPORTED, "earlyStopJohnson=true is not supported");
+    if (c->sorted_dfs) return fail(PBB_E_UNSUPPORTED, "sortedDFS != 0 is not supported");
+    if (c->nb_ivms < 1 || c->nb_ivms > (1 << 22)) return fail(PBB_E_INVAL, "nbIVMs must be in [1, 4194304]");
+    return PBB_OK;
+}
+
+int pbb_engine_destroy(pbb_engine* e)
+{
+    if (!e) return PBB_OK;
+    cudaSetDevice(e->dev);
+    if (e->st) cudaStreamSynchronize(e->st);
+    e->di.release();
+    cudaFree(e->mat); cudaFree(e->vec); cudaFree(e->bestperm);
+    cudaFree(e->line); cudaFree(e->state); cudaFree(e->bestcost); cudaFree(e->qval); cudaFree(e->qseq);
+    cudaFree(e->ub_d); cudaFree(e->root_d); cudaFree(e->ival_d); cudaFree(e->ctl); cudaFree(e->group_d);
+    if (e->ev0) cudaEventDestroy(e->ev0);
+    if (e->ev1) cudaEventDestroy(e->ev1);
+    if (e->st) cudaStreamDestroy(e->st);
+    delete e;
+    return PBB_OK;
+}
+
+static int engine_create(const pbb_instance* inst, const pbb_config* cfg, pbb_engine* e)
+{
+    e->cfg = *cfg;
+    int rc = check_config(cfg);
+    if (rc) return rc;
+    rc = build_tables(inst, cfg->johnson_mode, e->H);
+    if (rc) return rc;
+    e->dev = cfg->device;
+    CK(cudaSetDevice(e->dev));
+    CK(cudaStreamCreateWithFlags(&e->st, cudaStreamNonBlocking));
+    CK(cudaEventCreate(&e->ev0));
+    CK(cudaEventCreate(&e->ev1));
+    const HostTables& H = e->H;
+    e->nw = H.n <= 32 ? 1 : 2;
+    e->warps = pick_warps(H, cfg->warps_per_cta, e->dev, e->smem);
+    if (e->warps < 1) return fail(PBB_E_INVAL, "instance tables do not fit in shared memory");
+    e->root_smem = pbbl::smem_bytes(H.n, H.m, H.Ppad, 1);
+    int sms = 0;
+    CK(cudaDeviceGetAttribute(&sms, cudaDevAttrMultiProcessorCount, e->dev));
+    e->ctas = cfg->ctas > 0 ? cfg->ctas : sms;
+    rc = e->di.upload(H, e->st);
+    if (rc) return rc;
+    const int B = cfg->nb_ivms;
+    const int npad = PBB_MAX_N;
+    CK(cudaMalloc(&e->mat, (size_t)B * npad * npad));
+    CK(cudaMalloc(&e->vec, (size_t)B * npad * 4));
+    CK(cudaMalloc(&e->bestperm, (size_t)B * npad));
+    CK(cudaMalloc(&e->line, sizeof(int) * B));
+    CK(cudaMalloc(&e->state, sizeof(int) * B));
+    CK(cudaMalloc(&e->bestcost, sizeof(int) * B));
+    CK(cudaMalloc(&e->qval, sizeof(int) * B));
+    CK(cudaMalloc(&e->qseq, sizeof(unsigned) * B));
+    CK(cudaMalloc(&e->ub_d, sizeof(int)));
+    CK(cudaMalloc(&e->root_d, sizeof(int) * PBB_MAX_N));
+    CK(cudaMalloc(&e->ival_d, sizeof(int) * 2 * PBB_MAX_N));
+    CK(cudaMalloc(&e->ctl, sizeof(GroupCtl)));
+    CK(cudaMalloc(&e->group_d, sizeof(DevGroup)));
+    CK(cudaMemsetAsync(e->mat, 0, (size_t)B * npad * npad, e->st));
+    DevGroup& g = e->group;
+    g.inst = e->di.view;
+    g.search.bound_mode = cfg->bounding_mode;
+    g.search.branch_mode = cfg->branching_mode;
+    g.search.find_all = cfg->find_all ? 1 : 0;
+    g.ivm.count = B;
+    g.ivm.npad = npad;
+    g.ivm.mat = e->mat;
+    g.ivm.pos = e->vec;
+    g.ivm.end = e->vec + (size_t)B * npad;
+    g.ivm.dir = e->vec + (size_t)2 * B * npad;
+    g.ivm.pj = e->vec + (size_t)3 * B * npad;
+    g.ivm.line = e->line;
+    g.ivm.state = e->state;
+    g.ivm.bestcost = e->bestcost;
+    g.ivm.bestperm = e->bestperm;
+    g.ivm.qseq = e->qseq;
+    g.ivm.qval = e->qval;
+    g.ctl = e->ctl;
+    g.first_cta = 0;
+    g.ctas = e->ctas;
+    CK(cudaMemcpyAsync(e->group_d, &g, sizeof(DevGroup), cudaMemcpyHostToDevice, e->st));
+    CK(cudaStreamSynchronize(e->st));
+    return PBB_OK;
+}
+
+int pbb_engine_create(const pbb_instance* inst, const pbb_config* cfg, pbb_engine** out)
+{
+    if (!out) return fail(PBB_E_INVAL, "out is NULL");
+    *out = nullptr;
+    pbb_config def;
+    if (!cfg) { pbb_config_default(&def); cfg = &def; }
+    pbb_engine* e = new pbb_engine();
+    int rc = engine_create(inst, cfg, e);
+    if (rc) {
+        std::string keep = g_err;
+        pbb_engine_destroy(e);
+        g_err = keep;
+        return rc;
+    }
+    *out = e;
+    return PBB_OK;
+}
+
+static int start_impl(pbb_engine* e, int32_t ub, const int32_t* root_perm, const int32_t* pos, const int32_t* end)
+{
+    if (!e) return fail(PBB_E_INVAL, "engine is NULL");
+    CK(cudaSetDevice(e->dev));
+    const int n = e->H.n;
+    std::vector<int> root(PBB_MAX_N, 0);
+    std::vector<int> seen(n, 0);
+    for (int i = 0; i < n; i++) {
+        const int j = root_perm ? root_perm[i] : i;
+        if (j < 0 || j >= n || seen[j]) return fail(PBB_E_INVAL, "root_perm is not a permutation of 0..n-1");
+        seen[j] = 1;
+        root[i] = j;
+    }
+    // factoradic interval: digit i in [0, n-i) (sequentialbb.cpp:207-222 checks)
+    std::vector<int> iv(2 * PBB_MAX_N, 0);
+    for (int i = 0; i < n; i++) {
+        const int p = pos ? pos[i] : 0;
+        const int q = end ? end[i] : n - 1 - i;
+        if (p < 0 || p >= n - i || q < 0 || q >= n - i) return fail(PBB_E_INVAL, "interval digit out of range");
+        iv[i] = p;
+        iv[PBB_MAX_N + i] = q;
+    }
+    if (ub < 0) return fail(PBB_E_INVAL, "ub must be >= 0");
+    e->ub = ub;
+    CK(cudaMemcpyAsync(e->ub_d, &ub, sizeof(int), cudaMemcpyHostToDevice, e->st));
+    CK(cudaMemcpyAsync(e->root_d, root.data(), sizeof(int) * PBB_MAX_N, cudaMemcpyHostToDevice, e->st));
+    CK(cudaMemcpyAsync(e->ival_d, iv.data(), sizeof(int) * 2 * PBB_MAX_N, cudaMemcpyHostToDevice, e->st));
+    CK(pbbl::launch_reset(e->group_d, 1, e->ub_d, e->st));
+    CK(pbbl::launch_root(e->nw, e->group_d, 1, e->root_d, e->ival_d, PBB_MAX_N, e->root_smem, e->st));
+    CK(cudaStreamSynchronize(e->st));
+    GroupCtl c;
+    CK(cudaMemcpy(&c, e->ctl, sizeof(c), cudaMemcpyDeviceToHost));
+    e->started = true;
+    e->done = (c.active == 0);
+    e->dev_seconds = 0.0;
+    return PBB_OK;
+}
+
+int pbb_start(pbb_engine* e, int32_t ub, const int32_t* root_perm) { return start_impl(e, ub, root_perm, nullptr, nullptr); }
+
+int pbb_start_interval(pbb_engine* e, int32_t ub, const int32_t* root_perm, const int32_t* pos, const int32_t* end)
+{
+    if (!pos || !end) return fail(PBB_E_INVAL, "pos/end are NULL");
+    return start_impl(e, ub, root_perm, pos, end);
+}
+
+int pbb_set_ub(pbb_engine* e, int32_t ub)
+{
+    if (!e || !e->started) return fail(PBB_E_INVAL, "engine not started");
+    CK(cudaSetDevice(e->dev));
+    CK(pbbl::launch_lower_ub(e->group_d, 0, ub, e->st));
+    CK(cudaStreamSynchronize(e->st));
+    return PBB_OK;
+}
+
+int pbb_explore(pbb_engine* e, double seconds, int32_t* done)
+{
+    if (!e || !e->started) return fail(PBB_E_INVAL, "engine not started");
+    CK(cudaSetDevice(e->dev));
+    if (!e->done) {
+        // a launch never runs unbounded: at most 120 s of device time per window
+        const double win = (seconds > 0 && seconds < 120.0) ? seconds : 120.0;
+        const unsigned long long budget = (unsigned long long)(win * 1e9);
+        CK(cudaEventRecord(e->ev0, e->st));
+        CK(pbbl::launch_explore(e->nw, e->group_d, 1, e->ctas, e->warps, e->smem, budget, INT_MAX,
+                                e->select_budget, e->st));
+        CK(cudaEventRecord(e->ev1, e->st));
+        CK(pbbl::launch_requeue(e->group_d, 1, e->st));
+        CK(cudaStreamSynchronize(e->st));
+        float ms = 0.f;
+        CK(cudaEventElapsedTime(&ms, e->ev0, e->ev1));
+        e->dev_seconds += ms * 1e-3;
+        int active = 0;
+        CK(cudaMemcpy(&active, &e->ctl->active, sizeof(int), cudaMemcpyDeviceToHost));
+        e->done = (active == 0);
+    }
+    if (done) *done = e->done ? 1 : 0;
+    return PBB_OK;
+}
+
+int pbb_get_result(pbb_engine* e, pbb_result* out)
+{
+    if (!e || !out) return fail(PBB_E_INVAL, "NULL argument");
+    CK(cudaSetDevice(e->dev));
+    CK(cudaStreamSynchronize(e->st));
+    GroupCtl c;
+    CK(cudaMemcpy(&c, e->ctl, sizeof(c), cudaMemcpyDeviceToHost));
+    memset(out, 0, sizeof(*out));
+    out->complete = e->done ? 1 : 0;
+    const unsigned best_id = (unsigned)(c.best_key & 0xffffffffull);
+    // a bound lowered from outside (pbb_set_ub) carries no permutation here
+    out->found = (c.found > 0 && best_id != 0xffffffffu) ? 1 : 0;
+    out->cost = (int32_t)(c.best_key >> 32);
+    out->n_jobs = e->H.n;
+    out->stats.decomposed = c.decomposed;
+    out->stats.johnson_bounds = c.johnson_bounds;
+    out->stats.simple_bounds = c.simple_bounds;
+    out->stats.leaves = c.leaves;
+    out->stats.steals = c.steals;
+    out->device_seconds = e->dev_seconds;
+    if (c.status & PBB_ST_BADINPUT) return fail(PBB_E_INVAL, "device reported bad input");
+    if (out->found) {
+        const unsigned id = (unsigned)(c.best_key & 0xffffffffull);
+        if (id >= (unsigned)e->cfg.nb_ivms) return fail(PBB_E_CUDA, "corrupt best key");
+        signed char buf[PBB_MAX_N];
+        CK(cudaMemcpy(buf, e->bestperm + (size_t)id * PBB_MAX_N, PBB_MAX_N, cudaMemcpyDeviceToHost));
+        for (int i = 0; i < e->H.n; i++) out->perm[i] = buf[i];
+    }
+    return PBB_OK;
+}
+
+int pbb_solve(pbb_engine* e, int32_t ub, const int32_t* root_perm, double time_limit_s, pbb_result* out)
+{
+    int rc = pbb_start(e, ub, root_perm);
+    if (rc) return rc;
+    int32_t done = e->done ? 1 : 0;
+    while (!done) {
+        double slice = e->slice_s;
+        if (time_limit_s > 0) {
+            const double left = time_limit_s - e->dev_seconds;
+            if (left <= 0) break;
+            slice = std::min(slice, left);
+        }
+        rc = pbb_explore(e, slice, &done);
+        if (rc) return rc;
+    }
+    return pbb_get_result(e, out);
+}
+
+int pbb_bound_children(const pbb_instance* inst, int32_t johnson_mode, int32_t device, int32_t count,
+                       const int32_t* sched, const int32_t* limit1, const int32_t* limit2, int32_t* weak_begin,
+                       int32_t* weak_end, int32_t* strong_begin, int32_t* strong_end, int32_t* node_weak,
+                       int32_t* node_strong)
+{
+    if (count < 0 || (count > 0 && (!sched || !limit1 || !limit2))) return fail(PBB_E_INVAL, "bad node arrays");
+    HostTables H;
+    int rc = build_tables(inst, johnson_mode, H);
+    if (rc) return rc;
+    if (count == 0) return PBB_OK;
+    const int n = H.n;
+    for (int i = 0; i < count; i++) {
+        if (limit1[i] < -1 || limit2[i] > n || limit1[i] >= limit2[i]) return fail(PBB_E_INVAL, "bad limits");
+        std::vector<int> seen(n, 0);
+        for (int t = 0; t < n; t++) {
+            const int j = sched[(size_t)i * n + t];
+            if (j < 0 || j >= n || seen[j]) return fail(PBB_E_INVAL, "schedule is not a permutation");
+            seen[j] = 1;
+        }
+    }
+    CK(cudaSetDevice(device));
+    cudaStream_t st;
+    CK(cudaStreamCreateWithFlags(&st, cudaStreamNonBlocking));
+    DeviceInstance di;
+    rc = di.upload(H, st);
+    int* buf = nullptr;
+    unsigned* status = nullptr;
+    const size_t cn = (size_t)count * n;
+    const size_t words = cn * 5 + (size_t)count * 4;
+    do {
+        if (rc) break;
+        cudaError_t ce = cudaMalloc(&buf, sizeof(int) * words);
+        if (ce == cudaSuccess) ce = cudaMalloc(&status, sizeof(unsigned));
+        if (ce != cudaSuccess) { rc = cuda_fail(ce, "cudaMalloc"); break; }
+        int* d_s = buf;
+        int* d_wb = d_s + cn;
+        int* d_we = d_wb + cn;
+        int* d_sb = d_we + cn;
+        int* d_se = d_sb + cn;
+        int* d_l1 = d_se + cn;
+        int* d_l2 = d_l1 + count;
+        int* d_nw = d_l2 + count;
+        int* d_ns = d_nw + count;
+        cudaMemcpyAsync(d_s, sched, sizeof(int) * cn, cudaMemcpyHostToDevice, st);
+        cudaMemcpyAsync(d_l1, limit1, sizeof(int) * count, cudaMemcpyHostToDevice, st);
+        cudaMemcpyAsync(d_l2, limit2, sizeof(int) * count, cudaMemcpyHostToDevice, st);
+        cudaMemsetAsync(status, 0, sizeof(unsigned), st);
+        int smem = 0;
+        const int warps = pick_warps(H, 8, device, smem);
+        if (warps < 1) { rc = fail(PBB_E_INVAL, "instance tables do not fit in shared memory"); break; }
+        int sms = 0;
+        cudaDeviceGetAttribute(&sms, cudaDevAttrMultiProcessorCount, device);
+        int ctas = (count + warps - 1) / warps;
+        ctas = std::min(ctas, sms * 4);
+        ce = pbbl::launch_bound(n <= 32 ? 1 : 2, di.view, count, d_s, d_l1, d_l2, d_wb, d_we, d_sb, d_se, d_nw, d_ns,
+                                status, ctas, warps, smem, st);
+        if (ce != cudaSuccess) { rc = cuda_fail(ce, "pbb_bound_kernel launch"); break; }
+        if (weak_begin) cudaMemcpyAsync(weak_begin, d_wb, sizeof(int) * cn, cudaMemcpyDeviceToHost, st);
+        if (weak_end) cudaMemcpyAsync(weak_end, d_we, sizeof(int) * cn, cudaMemcpyDeviceToHost, st);
+        if (strong_begin) cudaMemcpyAsync(strong_begin, d_sb, sizeof(int) * cn, cudaMemcpyDeviceToHost, st);
+        if (strong_end) cudaMemcpyAsync(strong_end, d_se, sizeof(int) * cn, cudaMemcpyDeviceToHost, st);
+        if (node_weak) cudaMemcpyAsync(node_weak, d_nw, sizeof(int) * count, cudaMemcpyDeviceToHost, st);
+        if (node_strong) cudaMemcpyAsync(node_strong, d_ns, sizeof(int) * count, cudaMemcpyDeviceToHost, st);
+        unsigned hs = 0;
+        cudaMemcpyAsync(&hs, status, sizeof(unsigned), cudaMemcpyDeviceToHost, st);
+        ce = cudaStreamSynchronize(st);
+        if (ce != cudaSuccess) { rc = cuda_fail(ce, "pbb_bound_kernel"); break; }
+        if (hs & PBB_ST_BADINPUT) rc = fail(PBB_E_INVAL, "device rejected a node");
+    } while (0);
+    cudaFree(buf);
+    cudaFree(status);
+    di.release();
+    cudaStreamDestroy(st);
+    return rc;
+}
+
+int pbb_work_counters(pbb_engine* e, pbb_work* out)
+{
+    if (!e || !out) return fail(PBB_E_INVAL, "NULL argument");
+    CK(cudaSetDevice(e->dev));
+    CK(cudaStreamSynchronize(e->st));
+    GroupCtl c;
+    CK(cudaMemcpy(&c, e->ctl, sizeof(c), cudaMemcpyDeviceToHost));
+    out->device_seconds = e->dev_seconds;
+    out->n_jobs = e->H.n;
+    out->n_machines = e->H.m;
+    out->machine_pairs = e->H.P;
+    out->decomposed = c.decomposed;
+    out->simple_bounds = c.simple_bounds;
+    out->johnson_bounds = c.johnson_bounds;
+    out->johnson_sweeps = c.jsweeps;
+    out->sweep_free_jobs = c.jfree;
+    out->sweep_children = c.jchild;
+    out->explorers = e->cfg.nb_ivms;
+    out->warps = e->warps * e->ctas;
+    return PBB_OK;
+}
+
+// NEH (heuristic/src/fastNEH.cpp:230-243 for the insertion procedure): jobs
+// by decreasing total time (ties: lower id first); the first two keep the
+// swapped order unless the original one is strictly better; each next job is
+// inserted at the first position of least partial makespan.
+int pbb_neh(const pbb_instance* inst, int32_t* perm, int32_t* cost)
+{
+    if (!inst || !inst->p || !perm) return fail(PBB_E_INVAL, "NULL argument");
+    const int n = inst->n_jobs, m = inst->n_machines;
+    if (n < 1 || m < 1) return fail(PBB_E_INVAL, "empty instance");
+    const int32_t* p = inst->p;
+    std::vector<int> tot(n, 0), order(n);
+    for (int j = 0; j < n; j++) {
+        for (int k = 0; k < m; k++) tot[j] += p[k * n + j];
+        order[j] = j;
+    }
+    std::stable_sort(order.begin(), order.end(), [&](int a, int b) { return tot[a] > tot[b]; });
+    std::vector<int> c(m);
+    auto makespan = [&](const std::vector<int>& s) {
+        std::fill(c.begin(), c.end(), 0);
+        for (int j : s) {
+            c[0] += p[j];
+            for (int k = 1; k < m; k++) c[k] = std::max(c[k - 1], c[k]) + p[k * n + j];
+        }
+        return c[m - 1];
+    };
+    std::vector<int> seq;
+    if (n == 1) {
+        seq = {order[0]};
+    } else {
+        std::vector<int> a = {order[0], order[1]}, b = {order[1], order[0]};
+        seq = makespan(a) < makespan(b) ? a : b;
+        for (int k = 2; k < n; k++) {
+            int best = INT_MAX, bpos = 0;
+            std::vector<int> trial;
+            for (int q = 0; q <= k; q++) {
+                trial = seq;
+                trial.insert(trial.begin() + q, order[k]);
+                const int v = makespan(trial);
+                if (v < best) { best = v; bpos = q; }
+            }
+            seq.insert(seq.begin() + bpos, order[k]);
+        }
+    }
+    for (int i = 0; i < n; i++) perm[i] = seq[i];
+    if (cost) *cost = makespan(seq);
+    return PBB_OK;
+}
+
+}  // extern "C"

@@ -1,0 +1,850 @@
+// Kernels of the IVM flow-shop engine (sm_100a).
+//
+//   pbb_reset_kernel     explorers empty, idle queue and counters cleared
+//   pbb_root_kernel      root row bounded (weak, uncounted) + initial unfold
+//   pbb_explore_kernel   persistent explorer loop: select/decode/bound/prune
+//                        and work sharing through a device idle queue
+//   pbb_requeue_kernel   between launches: re-arm the idle queue
+//   pbb_bound_kernel     batched children bounds of given nodes (LB parity API)
+#include <cuda_runtime.h>
+#include <stdint.h>
+#include "pbb_types.h"
+#include "pbb_device.cuh"
+#include "pbb_launch.h"
+
+using namespace pbb;
+
+namespace {
+
+__device__ __forceinline__ unsigned long long globaltimer_ns()
+{
+    unsigned long long t;
+    asm volatile("mov.u64 %0, %%globaltimer;" : "=l"(t));
+    return t;
+}
+
+__device__ __forceinline__ int ld_acquire(const int* p)
+{
+    int v;
+    asm volatile("ld.acquire.gpu.global.s32 %0, [%1];" : "=r"(v) : "l"(p) : "memory");
+    return v;
+}
+
+__device__ __forceinline__ void st_release(int* p, int v)
+{
+    asm volatile("st.release.gpu.global.s32 [%0], %1;" ::"l"(p), "r"(v) : "memory");
+}
+
+__device__ __forceinline__ unsigned ld_acquire_u32(const unsigned* p)
+{
+    unsigned v;
+    asm volatile("ld.acquire.gpu.global.u32 %0, [%1];" : "=r"(v) : "l"(p) : "memory");
+    return v;
+}
+
+__device__ __forceinline__ void st_release_u32(unsigned* p, unsigned v)
+{
+    asm volatile("st.release.gpu.global.u32 [%0], %1;" ::"l"(p), "r"(v) : "memory");
+}
+
+__device__ __forceinline__ unsigned long long ld_volatile_u64(const unsigned long long* p)
+{
+    return *reinterpret_cast<const volatile unsigned long long*>(p);
+}
+
+__device__ __forceinline__ int ld_volatile_s32(const int* p) { return *reinterpret_cast<const volatile int*>(p); }
+
+// Load the group's instance tables into this CTA's shared memory.
+__device__ void load_tables(const DevInstance& I, unsigned char* smem, const SmemPlan& sp, CtaTables& T)
+{
+    const int tid = threadIdx.x, nt = blockDim.x;
+    unsigned long long* je = reinterpret_cast<unsigned long long*>(smem + sp.je_off);
+    int* p = reinterpret_cast<int*>(smem + sp.p_off);
+    unsigned char* pm0 = smem + sp.pm0_off;
+    unsigned char* pm1 = smem + sp.pm1_off;
+    int* marr = reinterpret_cast<int*>(smem + sp.marr_off);
+    int* mdep = reinterpret_cast<int*>(smem + sp.mdep_off);
+    for (int i = tid; i < I.n * I.Ppad; i += nt) je[i] = I.je[i];
+    for (int i = tid; i < I.n * I.m; i += nt) p[i] = I.p[i];
+    for (int i = tid; i < I.Ppad; i += nt) { pm0[i] = I.pm0[i]; pm1[i] = I.pm1[i]; }
+    for (int i = tid; i < I.m; i += nt) { marr[i] = I.min_arr[i]; mdep[i] = I.min_dep[i]; }
+    T.je = je; T.p = p; T.pm0 = pm0; T.pm1 = pm1; T.min_arr = marr; T.min_dep = mdep;
+    T.n = I.n; T.m = I.m; T.P = I.P; T.Ppad = I.Ppad;
+}
+
+// ---------------------------------------------------------------------------
+// explorer registers and their HBM image
+// ---------------------------------------------------------------------------
+template <int NW>
+struct Ivm {
+    int pos[NW], end[NW], dir[NW], pj[NW], row[NW];
+    int line;
+};
+
+__device__ __forceinline__ signed char* mat_row(const DevIvms& V, int id, int l)
+{
+    return V.mat + ((size_t)id * V.npad + l) * V.npad;
+}
+
+template <int NW>
+__device__ __forceinline__ void load_row(const DevIvms& V, int id, int l, int (&row)[NW])
+{
+    const signed char* r = mat_row(V, id, l);
+#pragma unroll
+    for (int w = 0; w < NW; w++) row[w] = __ldcg(r + w * 32 + lane_id());
+}
+
+template <int NW>
+__device__ __forceinline__ void store_row(const DevIvms& V, int id, int l, const int (&row)[NW])
+{
+    signed char* r = mat_row(V, id, l);
+#pragma unroll
+    for (int w = 0; w < NW; w++) __stcg(r + w * 32 + lane_id(), (signed char)row[w]);
+}
+
+template <int NW>
+__device__ __forceinline__ void load_ivm(const DevIvms& V, int id, Ivm<NW>& R)
+{
+    const size_t b = (size_t)id * V.npad;
+#pragma unroll
+    for (int w = 0; w < NW; w++) {
+        const int e = w * 32 + lane_id();
+        R.pos[w] = __ldcg(V.pos + b + e);
+        R.end[w] = __ldcg(V.end + b + e);
+        R.dir[w] = __ldcg(V.dir + b + e);
+        R.pj[w] = __ldcg(V.pj + b + e);
+    }
+    R.line = __ldcg(V.line + id);
+    load_row<NW>(V, id, R.line, R.row);
+}
+
+template <int NW>
+__device__ __forceinline__ void store_ivm(const DevIvms& V, int id, const Ivm<NW>& R)
+{
+    const size_t b = (size_t)id * V.npad;
+#pragma unroll
+    for (int w = 0; w < NW; w++) {
+        const int e = w * 32 + lane_id();
+        __stcg(V.pos + b + e, (signed char)R.pos[w]);
+        __stcg(V.end + b + e, (signed char)R.end[w]);
+        __stcg(V.dir + b + e, (signed char)R.dir[w]);
+        __stcg(V.pj + b + e, (signed char)R.pj[w]);
+    }
+    if (lane_id() == 0) __stcg(V.line + id, R.line);
+}
+
+// front / back job lists of the current path (ivm_bound.cpp:112-138)
+template <int NW>
+__device__ __forceinline__ void build_lists(const WarpScratch& S, const Ivm<NW>& R, int L, int& f, int& b)
+{
+    f = 0; b = 0;
+#pragma unroll
+    for (int w = 0; w < NW; w++) {
+        const int lv = w * 32 + lane_id();
+        const bool isF = lv < L && R.dir[w] == 0;
+        const bool isB = lv < L && R.dir[w] != 0;
+        const unsigned bf = __ballot_sync(FULLMASK, isF), bb = __ballot_sync(FULLMASK, isB);
+        if (isF) S.fjob[f + __popc(bf & lanemask_lt())] = (unsigned char)R.pj[w];
+        if (isB) S.bjob[b + __popc(bb & lanemask_lt())] = (unsigned char)R.pj[w];
+        f += __popc(bf);
+        b += __popc(bb);
+    }
+    __syncwarp();
+}
+
+struct WarpCounters {
+    unsigned long long decomposed, simple, johnson, leaves;
+    unsigned long long sweeps, free_jobs, swept_children;
+};
+
+// Record an improving leaf: permutation into the explorer's slot, then the
+// (cost, explorer) key into the group's best (solution.cpp:27-45 restated as
+// a packed atomicMin instead of a mutex).
+template <int NW>
+__device__ void record_solution(const DevGroup& G, const WarpScratch& S, int id, int f, int b, int last, int cost)
+{
+    const int n = G.inst.n;
+    signed char* slot = G.ivm.bestperm + (size_t)id * G.ivm.npad;
+    for (int i = lane_id(); i < n; i += 32) {
+        int j;
+        if (i < f) j = S.fjob[i];
+        else if (i == f) j = last;
+        else j = S.bjob[n - 1 - i];
+        slot[i] = (signed char)j;
+    }
+    __syncwarp();
+    if (lane_id() == 0) {
+        G.ivm.bestcost[id] = cost;
+        __threadfence();
+        atomicMin(&G.ctl->best_key, ((unsigned long long)(unsigned)cost << 32) | (unsigned)id);
+        atomicAdd(&G.ctl->found, 1);
+    }
+    __syncwarp();
+}
+
+// One call of sequentialbb::next (multicore/src/sequentialbb.cpp:110-190):
+// advance to the next unpruned node of the interval, evaluating leaves on the
+// way.  Returns 1 with a node to bound at R.line, 0 when the interval is
+// exhausted, 2 when the selection budget ran out (state stays consistent).
+template <int NW>
+__device__ int select_node(const DevGroup& G, const CtaTables& T, const WarpScratch& S, int id, Ivm<NW>& R,
+                           int& best, WarpCounters& C, int budget)
+{
+    const int n = T.n;
+    const bool fa = G.search.find_all != 0;
+    for (int it = 0; it < budget; it++) {
+        if (!before_end<NW>(R.pos, R.end, n)) return 0;
+        int L = R.line;
+        const int k = n - L;
+        const int p = vget<NW>(R.pos, L);
+        if (p >= k) {                                    // goUp (ivm.cpp:97-112)
+            if (L > 0) {
+                vset<NW>(R.pos, L, 0);
+                L--;
+                R.line = L;
+                load_row<NW>(G.ivm, id, L, R.row);
+                const int pp = vget<NW>(R.pos, L);
+                if (lane_id() == (pp & 31)) {
+#pragma unroll
+                    for (int w = 0; w < NW; w++)
+                        if ((pp >> 5) == w) {
+                            R.row[w] = cell_flag(R.row[w]);
+                            __stcg(mat_row(G.ivm, id, L) + pp, (signed char)R.row[w]);
+                        }
+                }
+            } else {
+                vset<NW>(R.pos, 0, p + 1);
+            }
+            continue;
+        }
+        const int c = next_open_cell<NW>(R.row, p, k);   // goRight over pruned cells
+        if (c != p) {
+            vset<NW>(R.pos, L, c);
+            continue;
+        }
+        // goDown (ivm.cpp:114-173): the node at (L, p) is decomposed
+        C.decomposed++;
+        const int u = vget<NW>(R.row, p);
+        vset<NW>(R.pj, L, u);
+        int nr[NW];
+#pragma unroll
+        for (int w = 0; w < NW; w++) {
+            const int idx = w * 32 + lane_id();
+            int src = idx < p ? idx : idx + 1;
+            if (src >= 32 * NW) src = 0;
+            nr[w] = cell_job(vgather<NW>(R.row, src));
+        }
+#pragma unroll
+        for (int w = 0; w < NW; w++) R.row[w] = nr[w];
+        L++;
+        R.line = L;
+        vset<NW>(R.pos, L, 0);
+        vset<NW>(R.dir, L, 0);
+        if (L == n - 1) {                                 // leaf (ivm_bound.cpp:239-271)
+            C.leaves++;
+            int f, b;
+            build_lists<NW>(S, R, L, f, b);
+            const int last = vget<NW>(R.row, 0);
+            if (lane_id() == 0) S.rowj[0] = (unsigned char)last;
+            __syncwarp();
+            partial_schedule(T, S, f, b, 1);
+            int cost = 0;
+            if (lane_id() == 0) cost = makespan_split(T, S, last, -1);
+            cost = __shfl_sync(FULLMASK, cost, 0);
+            const bool better = fa ? !(cost > best) : !(cost >= best);
+            if (better) {
+                best = cost;
+                record_solution<NW>(G, S, id, f, b, last, cost);
+            }
+            if (lane_id() == 0) {
+                R.row[0] = cell_flag(R.row[0]);
+                __stcg(mat_row(G.ivm, id, L), (signed char)R.row[0]);
+            }
+            continue;
+        }
+        return 1;
+    }
+    return 2;
+}
+
+// Bound and prune the node selected at R.line and write its row back.
+template <int NW>
+__device__ __forceinline__ void bound_current(const DevGroup& G, const CtaTables& T, const WarpScratch& S, int id,
+                                              Ivm<NW>& R, int mode, int best, WarpCounters& C)
+{
+    const int L = R.line;
+    int f, b;
+    build_lists<NW>(S, R, L, f, b);
+    const int prev = L > 0 ? vget<NW>(R.dir, L - 1) : 0;
+    NodeCounters nc = {0, 0, 0, 0, 0};
+    const int d = bound_and_prune<NW>(T, S, G.search, mode, R.row, T.n - L, f, b, L, prev, best, nc);
+    vset<NW>(R.dir, L, d);
+    store_row<NW>(G.ivm, id, L, R.row);
+    C.simple += nc.simple;
+    C.johnson += nc.johnson;
+    C.sweeps += nc.sweeps;
+    C.free_jobs += nc.free_jobs;
+    C.swept_children += nc.swept_children;
+}
+
+// ---------------------------------------------------------------------------
+// idle-explorer queue: bounded MPMC queue with per-cell sequence numbers
+// (D. Vyukov's design), one lane operates it
+// ---------------------------------------------------------------------------
+__device__ bool queue_push(const DevGroup& G, int v)
+{
+    const unsigned long long cap = (unsigned long long)G.ivm.count;
+    for (int attempt = 0; attempt < 64; attempt++) {
+        unsigned long long pos = ld_volatile_u64(&G.ctl->q_tail);
+        const int cell = (int)(pos % cap);
+        const unsigned seq = ld_acquire_u32(G.ivm.qseq + cell);
+        const int dif = (int)(seq - (unsigned)pos);
+        if (dif == 0) {
+            if (atomicCAS(&G.ctl->q_tail, pos, pos + 1) == pos) {
+                G.ivm.qval[cell] = v;
+                st_release_u32(G.ivm.qseq + cell, (unsigned)(pos + 1));
+                return true;
+            }
+        } else if (dif < 0) {
+            return false;
+        }
+    }
+    return false;
+}
+
+__device__ int queue_pop(const DevGroup& G)
+{
+    const unsigned long long cap = (unsigned long long)G.ivm.count;
+    for (int attempt = 0; attempt < 64; attempt++) {
+        unsigned long long pos = ld_volatile_u64(&G.ctl->q_head);
+        const int cell = (int)(pos % cap);
+        const unsigned seq = ld_acquire_u32(G.ivm.qseq + cell);
+        const int dif = (int)(seq - (unsigned)(pos + 1));
+        if (dif == 0) {
+            if (atomicCAS(&G.ctl->q_head, pos, pos + 1) == pos) {
+                const int v = __ldcg(G.ivm.qval + cell);
+                st_release_u32(G.ivm.qseq + cell, (unsigned)(pos + cap));
+                return v;
+            }
+        } else if (dif < 0) {
+            return -1;
+        }
+    }
+    return -1;
+}
+
+// Split the explorer's interval with a queued idle explorer
+// (bbthread::shareWork multicore/src/bbthread.cpp:40-72 and
+// ivm::cuttingPosition multicore/src/ivm.cpp:199-237): the first level l where
+// pos and end differ (not below the current line, not deeper than n-10) is
+// cut so that the donor keeps half of the explorable cells after pos[l]; the
+// receiver gets rows 0..l and the right part, and continues with next()
+// without an uncounted unfold, so decomposed-node counts do not depend on
+// how the work was shared.
+template <int NW>
+__device__ void try_share(const DevGroup& G, int id, Ivm<NW>& R)
+{
+    const int n = G.inst.n;
+    // cheap emptiness test of the queue first
+    if (ld_volatile_u64(&G.ctl->q_tail) == ld_volatile_u64(&G.ctl->q_head)) return;
+    int f = n;
+#pragma unroll
+    for (int w = NW - 1; w >= 0; w--) {
+        const int lv = w * 32 + lane_id();
+        const unsigned d = __ballot_sync(FULLMASK, lv < n && R.pos[w] != R.end[w]);
+        if (d) f = w * 32 + __ffs(d) - 1;
+    }
+    const int lcap = n - 10 > 0 ? n - 10 : 0;
+    int l = f;
+    if (l > R.line) l = R.line;
+    if (l > lcap) l = lcap;
+    const int pl = vget<NW>(R.pos, l), el = vget<NW>(R.end, l);
+    if (!(pl < el)) return;
+    int thief = -1;
+    if (lane_id() == 0) thief = queue_pop(G);
+    thief = __shfl_sync(FULLMASK, thief, 0);
+    if (thief < 0) return;
+
+    int row[NW];
+    if (l == R.line) {
+#pragma unroll
+        for (int w = 0; w < NW; w++) row[w] = R.row[w];
+    } else {
+        load_row<NW>(G.ivm, id, l, row);
+    }
+    // cutting position: keep = explorable / 2 cells after pos[l]
+    int expl = 0;
+    unsigned em[NW];
+#pragma unroll
+    for (int w = 0; w < NW; w++) {
+        const int idx = w * 32 + lane_id();
+        em[w] = __ballot_sync(FULLMASK, idx > pl && idx <= el && row[w] >= 0);
+        expl += __popc(em[w]);
+    }
+    const int keep = expl / 2;
+    int cut = pl + 1;
+    if (keep > 0) {
+        int rem = keep;
+#pragma unroll
+        for (int w = 0; w < NW; w++) {
+            const int c = __popc(em[w]);
+            if (rem > 0 && rem <= c) {
+                unsigned msk = em[w];
+                for (int r = 1; r < rem; r++) msk &= msk - 1;
+                cut = w * 32 + __ffs(msk) - 1 + 1;
+                rem = 0;
+            } else if (rem > 0) {
+                rem -= c;
+            }
+        }
+    }
+    // receiver image
+    const size_t tb = (size_t)thief * G.ivm.npad;
+    const int* src = reinterpret_cast<const int*>(mat_row(G.ivm, id, 0));
+    int* dst = reinterpret_cast<int*>(mat_row(G.ivm, thief, 0));
+    const int words = (l + 1) * G.ivm.npad / 4;
+    for (int i = lane_id(); i < words; i += 32) __stcg(dst + i, __ldcg(src + i));
+#pragma unroll
+    for (int w = 0; w < NW; w++) {
+        const int lv = w * 32 + lane_id();
+        const int tp = lv < l ? R.pos[w] : (lv == l ? cut : 0);
+        __stcg(G.ivm.pos + tb + lv, (signed char)tp);
+        __stcg(G.ivm.end + tb + lv, (signed char)R.end[w]);
+        __stcg(G.ivm.dir + tb + lv, (signed char)(lv <= l ? R.dir[w] : 0));
+        __stcg(G.ivm.pj + tb + lv, (signed char)(lv < l ? R.pj[w] : 0));
+    }
+    if (lane_id() == 0) __stcg(G.ivm.line + thief, l);
+    // donor keeps [pos, cut-1] at level l, everything below l
+#pragma unroll
+    for (int w = 0; w < NW; w++) {
+        const int lv = w * 32 + lane_id();
+        if (lv == l) R.end[w] = cut - 1;
+        else if (lv > l) R.end[w] = n - 1 - lv;
+    }
+    __threadfence();
+    __syncwarp();
+    if (lane_id() == 0) {
+        atomicAdd(&G.ctl->active, 1);
+        atomicAdd(&G.ctl->steals, 1ull);
+        st_release(G.ivm.state + thief, IVM_ACTIVE);
+    }
+    __syncwarp();
+}
+
+__device__ __forceinline__ int group_of_cta(const DevGroup* groups, int ngroups)
+{
+    int lo = 0, hi = ngroups - 1;
+    const int c = blockIdx.x;
+    while (lo < hi) {
+        int mid = (lo + hi + 1) >> 1;
+        if (groups[mid].first_cta <= c) lo = mid; else hi = mid - 1;
+    }
+    return lo;
+}
+
+}  // namespace
+
+// ---------------------------------------------------------------------------
+// kernels
+// ---------------------------------------------------------------------------
+
+// Empty every explorer of every group; clear counters and queues.
+__global__ void pbb_reset_kernel(const DevGroup* groups, int ngroups, const int* ub)
+{
+    for (int g = blockIdx.y; g < ngroups; g += gridDim.y) {
+        const DevGroup G = groups[g];
+        const int n = G.inst.n;
+        for (int id = blockIdx.x * blockDim.x + threadIdx.x; id < G.ivm.count; id += gridDim.x * blockDim.x) {
+            G.ivm.state[id] = IVM_IDLE;
+            G.ivm.line[id] = 0;
+            G.ivm.bestcost[id] = 0x7fffffff;
+            G.ivm.qseq[id] = (unsigned)id;
+            const size_t b = (size_t)id * G.ivm.npad;
+            for (int e = 0; e < G.ivm.npad; e++) {
+                G.ivm.pos[b + e] = 0;
+                G.ivm.end[b + e] = 0;
+                G.ivm.dir[b + e] = 0;
+                G.ivm.pj[b + e] = 0;
+            }
+            G.ivm.pos[b] = (signed char)n;   // empty interval (ivm.cpp:70-76)
+        }
+        if (blockIdx.x == 0 && threadIdx.x == 0) {
+            GroupCtl* c = G.ctl;
+            c->best_key = ((unsigned long long)(unsigned)ub[g] << 32) | 0xffffffffull;
+            c->active = 0; c->found = 0; c->status = 0;
+            c->decomposed = c->johnson_bounds = c->simple_bounds = c->leaves = c->root_simple = 0;
+            c->q_head = c->q_tail = 0; c->steals = 0;
+            c->jsweeps = c->jfree = c->jchild = 0;
+        }
+    }
+}
+
+// Root of each group (one warp per group): row 0 = root permutation, bounded
+// with the weak bound and pruned without counting (ivm_bound::boundRoot
+// ivm_bound.cpp:274-336, stats reset by initAtInterval sequentialbb.cpp:84-106),
+// then the uncounted descent along the interval start (unfold :207-264).
+template <int NW>
+__global__ void pbb_root_kernel(const DevGroup* groups, int ngroups, const int* roots, const int* ivals,
+                                int root_stride)
+{
+    extern __shared__ __align__(16) unsigned char smem[];
+    const int g = blockIdx.x;
+    if (g >= ngroups) return;
+    const DevGroup G = groups[g];
+    const SmemPlan sp = pbb_smem_plan(G.inst.n, G.inst.m, G.inst.Ppad, 1);
+    CtaTables T;
+    load_tables(G.inst, smem, sp, T);
+    __syncthreads();
+    const WarpScratch S = warp_scratch(smem + sp.warp_off, T.m);
+    const int n = T.n;
+    const int id = 0;
+    Ivm<NW> R;
+#pragma unroll
+    for (int w = 0; w < NW; w++) {
+        const int e = w * 32 + lane_id();
+        // interval [pos, end] of the group (initAtInterval sequentialbb.cpp:84-106)
+        R.pos[w] = e < n ? ivals[(2 * g) * root_stride + e] : 0;
+        R.end[w] = e < n ? ivals[(2 * g + 1) * root_stride + e] : 0;
+        R.dir[w] = 0;
+        R.pj[w] = 0;
+        R.row[w] = e < n ? roots[g * root_stride + e] : 0;
+    }
+    R.line = 0;
+    int best = (int)(G.ctl->best_key >> 32);
+    NodeCounters rootc = {0, 0, 0, 0, 0};
+    {
+        int f = 0, b = 0;
+        DevSearch weak = G.search;
+        const int d = bound_and_prune<NW>(T, S, weak, 0, R.row, n, f, b, 0, 0, best, rootc);
+        vset<NW>(R.dir, 0, d);
+    }
+    store_row<NW>(G.ivm, id, 0, R.row);
+    NodeCounters nc = {0, 0, 0, 0, 0};
+    const int mode = G.search.bound_mode;
+    while (R.line < n - 2) {
+        const int L = R.line;
+        const int p = vget<NW>(R.pos, L);
+        if (vget<NW>(R.row, p) < 0) break;             // pos below L are already 0
+        vset<NW>(R.pj, L, vget<NW>(R.row, p));
+        int nr[NW];
+#pragma unroll
+        for (int w = 0; w < NW; w++) {
+            const int idx = w * 32 + lane_id();
+            int src = idx < p ? idx : idx + 1;
+            if (src >= 32 * NW) src = 0;
+            nr[w] = cell_job(vgather<NW>(R.row, src));
+        }
+#pragma unroll
+        for (int w = 0; w < NW; w++) R.row[w] = nr[w];
+        R.line = L + 1;
+        int f, b;
+        build_lists<NW>(S, R, R.line, f, b);
+        const int prev = vget<NW>(R.dir, L);
+        const int d = bound_and_prune<NW>(T, S, G.search, mode, R.row, n - R.line, f, b, R.line, prev, best, nc);
+        vset<NW>(R.dir, R.line, d);
+        store_row<NW>(G.ivm, id, R.line, R.row);
+    }
+    store_ivm<NW>(G.ivm, id, R);
+    const bool alive = before_end<NW>(R.pos, R.end, n);
+    if (lane_id() == 0) {
+        G.ctl->simple_bounds += nc.simple;
+        G.ctl->johnson_bounds += nc.johnson;
+        G.ctl->root_simple += rootc.simple;
+        G.ctl->jsweeps += nc.sweeps;
+        G.ctl->jfree += nc.free_jobs;
+        G.ctl->jchild += nc.swept_children;
+        if (alive) {
+            G.ctl->active = 1;
+            G.ivm.state[id] = IVM_ACTIVE;
+        }
+    }
+}
+
+// Persistent explorer loop.  Warp w of a group serves explorers w, w+W, ...
+// (W = warps of the group).  Runs until no explorer of the group holds work,
+// or `budget_ns` of device time has passed, or `max_rounds` rounds.
+template <int NW>
+__global__ void __launch_bounds__(32 * PBB_WARPS_MAX, 1)
+pbb_explore_kernel(const DevGroup* groups, int ngroups, int warps_per_cta, unsigned long long budget_ns,
+                   int max_rounds, int select_budget)
+{
+    extern __shared__ __align__(16) unsigned char smem[];
+    const int gi = group_of_cta(groups, ngroups);
+    const DevGroup G = groups[gi];
+    const SmemPlan sp = pbb_smem_plan(G.inst.n, G.inst.m, G.inst.Ppad, warps_per_cta);
+    CtaTables T;
+    load_tables(G.inst, smem, sp, T);
+    __syncthreads();
+    const int wic = threadIdx.x >> 5;
+    const WarpScratch S = warp_scratch(smem + sp.warp_off + wic * sp.warp_bytes, T.m);
+    const int W = G.ctas * warps_per_cta;
+    const int wid = (blockIdx.x - G.first_cta) * warps_per_cta + wic;
+    const int mode = G.search.bound_mode;
+    const unsigned long long t0 = globaltimer_ns();
+
+    WarpCounters C = {0, 0, 0, 0, 0, 0, 0};
+    Ivm<NW> R;
+    int cached = -1;                   // explorer whose state is held in registers
+    const bool single = (G.ivm.count <= W);
+    int best = (int)(ld_volatile_u64(&G.ctl->best_key) >> 32);
+
+    for (int round = 0; round < max_rounds; round++) {
+        if (ld_volatile_s32(&G.ctl->active) == 0) break;
+        if (globaltimer_ns() - t0 > budget_ns) break;
+        bool worked = false;
+        for (int id = wid; id < G.ivm.count; id += W) {
+            int st = 0;
+            if (lane_id() == 0) st = ld_acquire(G.ivm.state + id);
+            st = __shfl_sync(FULLMASK, st, 0);
+            if (st == IVM_ACTIVE) {
+                if (cached != id) load_ivm<NW>(G.ivm, id, R);
+                cached = id;
+                const int gb = (int)(ld_volatile_u64(&G.ctl->best_key) >> 32);
+                if (gb < best) best = gb;
+                try_share<NW>(G, id, R);
+                const int r = select_node<NW>(G, T, S, id, R, best, C, select_budget);
+                if (r == 1) bound_current<NW>(G, T, S, id, R, mode, best, C);
+                worked = true;
+                if (r == 0) {
+                    // interval exhausted: leave the pool of busy explorers
+                    __syncwarp();
+                    cached = -1;
+                    if (lane_id() == 0) {
+                        st_release(G.ivm.state + id, IVM_QUEUED);
+                        atomicSub(&G.ctl->active, 1);
+                        if (!queue_push(G, id)) st_release(G.ivm.state + id, IVM_IDLE);
+                    }
+                    __syncwarp();
+                } else if (!single) {
+                    store_ivm<NW>(G.ivm, id, R);
+                    cached = -1;
+                }
+            } else if (st == IVM_IDLE) {
+                if (lane_id() == 0) {
+                    st_release(G.ivm.state + id, IVM_QUEUED);
+                    if (!queue_push(G, id)) st_release(G.ivm.state + id, IVM_IDLE);
+                }
+                __syncwarp();
+            }
+        }
+        if (!worked) __nanosleep(1000);
+    }
+    if (cached >= 0) store_ivm<NW>(G.ivm, cached, R);
+    if (lane_id() == 0) {
+        atomicAdd(&G.ctl->decomposed, C.decomposed);
+        atomicAdd(&G.ctl->simple_bounds, C.simple);
+        atomicAdd(&G.ctl->johnson_bounds, C.johnson);
+        atomicAdd(&G.ctl->leaves, C.leaves);
+        atomicAdd(&G.ctl->jsweeps, C.sweeps);
+        atomicAdd(&G.ctl->jfree, C.free_jobs);
+        atomicAdd(&G.ctl->jchild, C.swept_children);
+    }
+}
+
+// Lower a group's incumbent to `ub` (bound found elsewhere, no permutation here).
+__global__ void pbb_lower_ub_kernel(const DevGroup* groups, int g, int ub)
+{
+    atomicMin(&groups[g].ctl->best_key, ((unsigned long long)(unsigned)ub << 32) | 0xffffffffull);
+}
+
+// Between two launches: explorers waiting in the queue become idle again and
+// the queue is emptied (the next launch re-registers them).
+__global__ void pbb_requeue_kernel(const DevGroup* groups, int ngroups)
+{
+    for (int g = blockIdx.y; g < ngroups; g += gridDim.y) {
+        const DevGroup G = groups[g];
+        for (int id = blockIdx.x * blockDim.x + threadIdx.x; id < G.ivm.count; id += gridDim.x * blockDim.x) {
+            if (G.ivm.state[id] != IVM_ACTIVE) G.ivm.state[id] = IVM_IDLE;
+            G.ivm.qseq[id] = (unsigned)id;
+        }
+        if (blockIdx.x == 0 && threadIdx.x == 0) { G.ctl->q_head = 0; G.ctl->q_tail = 0; }
+    }
+}
+
+// Children bounds of `count` nodes (warp per node): weak LBs of every free job
+// appended at the front / back (bound_fsp_weak::boundChildren), Johnson LBs
+// of the same children (bound_fsp_strong::bornes_calculer on the child), the
+// node's own weak and Johnson LB, all indexed by job id (0 for fixed jobs).
+template <int NW>
+__global__ void pbb_bound_kernel(DevInstance I, int count, const int* sched, const int* l1s, const int* l2s,
+                                 int* wb, int* we, int* sb, int* se, int* node_weak, int* node_strong,
+                                 unsigned int* status, int warps_per_cta)
+{
+    extern __shared__ __align__(16) unsigned char smem[];
+    const SmemPlan sp = pbb_smem_plan(I.n, I.m, I.Ppad, warps_per_cta);
+    CtaTables T;
+    load_tables(I, smem, sp, T);
+    __syncthreads();
+    const int wic = threadIdx.x >> 5;
+    const WarpScratch S = warp_scratch(smem + sp.warp_off + wic * sp.warp_bytes, T.m);
+    const int n = T.n;
+    const int lane = lane_id();
+    for (int node = blockIdx.x * warps_per_cta + wic; node < count; node += gridDim.x * warps_per_cta) {
+        const int* s = sched + (size_t)node * n;
+        const int l1 = l1s[node], l2 = l2s[node];
+        const bool ok = l1 >= -1 && l2 <= n && l1 < l2;
+        if (!ok) {
+            if (lane == 0) atomicOr(status, PBB_ST_BADINPUT);
+            continue;
+        }
+        const int f = l1 + 1, b = n - l2, k = l2 - l1 - 1;
+        for (int i = lane; i < f; i += 32) S.fjob[i] = (unsigned char)s[i];
+        for (int i = lane; i < b; i += 32) S.bjob[i] = (unsigned char)s[n - 1 - i];
+        int row[NW];
+        bool valid[NW];
+#pragma unroll
+        for (int w = 0; w < NW; w++) {
+            const int idx = w * 32 + lane;
+            valid[w] = idx < k;
+            row[w] = valid[w] ? s[l1 + 1 + idx] : 0;
+            if (valid[w]) S.rowj[idx] = (unsigned char)row[w];
+        }
+        __syncwarp();
+        partial_schedule(T, S, f, b, k);
+        int* owb = wb + (size_t)node * n;
+        int* owe = we + (size_t)node * n;
+        int* osb = sb + (size_t)node * n;
+        int* ose = se + (size_t)node * n;
+        for (int i = lane; i < n; i += 32) { owb[i] = 0; owe[i] = 0; osb[i] = 0; ose[i] = 0; }
+        __syncwarp();
+#pragma unroll
+        for (int w = 0; w < NW; w++) {
+            if (valid[w]) {
+                owb[row[w]] = weak_front(T, S, row[w]);
+                owe[row[w]] = weak_back(T, S, row[w]);
+            }
+        }
+        const int wn = weak_node_lb(T, S);
+        // node Johnson LB and children Johnson LBs
+        int snode = 0;
+        unsigned um[NW];
+        job_mask<NW>(um, row, valid);
+        const int x0 = vget<NW>(row, 0);
+        const int x1 = vget<NW>(row, 1);
+        if (k <= 1) {
+            // at most one free job: the reference evaluates the full permutation
+            int v = 0;
+            if (lane == 0) {
+                if (k == 1) {
+                    v = makespan_split(T, S, x0, -1);
+                } else {
+                    for (int kk = 0; kk < T.m; kk++) v = max(v, S.frontZ[kk] + S.backZ[kk]);
+                }
+            }
+            snode = __shfl_sync(FULLMASK, v, 0);
+            // the one child on either side completes the permutation: its makespan
+            if (k == 1 && lane == 0) { osb[x0] = snode; ose[x0] = snode; }
+        } else {
+            if (k == 2) {
+                int mk = 0;
+                if (lane < 2) mk = makespan_split(T, S, lane == 0 ? x0 : x1, lane == 0 ? x1 : x0);
+                const int mxy = __shfl_sync(FULLMASK, mk, 0), myx = __shfl_sync(FULLMASK, mk, 1);
+#pragma unroll
+                for (int w = 0; w < NW; w++) {
+                    if (valid[w]) {
+                        osb[row[w]] = (row[w] == x0) ? mxy : myx;
+                        ose[row[w]] = (row[w] == x0) ? myx : mxy;
+                    }
+                }
+            }
+            for (int i = lane; i < PBB_MAX_N; i += 32) { S.lbF[i] = 0; S.lbB[i] = 0; }
+            __syncwarp();
+            const bool kids = k >= 3;
+            unsigned none[NW];
+#pragma unroll
+            for (int q = 0; q < NW; q++) none[q] = 0;
+            if (kids) child_tables<NW>(T, S, row, k, true, um, true, um);
+            int nl = 0;
+            if (kids) johnson_children<NW>(T, S, um, true, um, true, um, &nl);
+            else johnson_children<NW>(T, S, um, false, none, false, none, &nl);
+            snode = nl;
+            if (kids) {
+#pragma unroll
+                for (int w = 0; w < NW; w++) {
+                    if (valid[w]) {
+                        osb[row[w]] = S.lbF[row[w]];
+                        ose[row[w]] = S.lbB[row[w]];
+                    }
+                }
+            }
+        }
+        if (lane == 0) {
+            node_weak[node] = wn;
+            node_strong[node] = snode;
+        }
+        __syncwarp();
+    }
+}
+
+// ---------------------------------------------------------------------------
+// host-side launch wrappers (pbb_launch.h)
+// ---------------------------------------------------------------------------
+namespace pbbl {
+
+int smem_bytes(int n, int m, int Ppad, int warps) { return pbb_smem_plan(n, m, Ppad, warps).total; }
+
+cudaError_t launch_reset(const DevGroup* groups, int ngroups, const int* ub, cudaStream_t st)
+{
+    dim3 grid(64, ngroups < 65535 ? ngroups : 65535);
+    pbb_reset_kernel<<<grid, 256, 0, st>>>(groups, ngroups, ub);
+    return cudaGetLastError();
+}
+
+cudaError_t launch_root(int nw, const DevGroup* groups, int ngroups, const int* roots, const int* ivals,
+                        int root_stride, int smem, cudaStream_t st)
+{
+    if (nw == 1) {
+        cudaFuncSetAttribute(pbb_root_kernel<1>, cudaFuncAttributeMaxDynamicSharedMemorySize, smem);
+        pbb_root_kernel<1><<<ngroups, 32, smem, st>>>(groups, ngroups, roots, ivals, root_stride);
+    } else {
+        cudaFuncSetAttribute(pbb_root_kernel<2>, cudaFuncAttributeMaxDynamicSharedMemorySize, smem);
+        pbb_root_kernel<2><<<ngroups, 32, smem, st>>>(groups, ngroups, roots, ivals, root_stride);
+    }
+    return cudaGetLastError();
+}
+
+cudaError_t launch_lower_ub(const DevGroup* groups, int g, int ub, cudaStream_t st)
+{
+    pbb_lower_ub_kernel<<<1, 1, 0, st>>>(groups, g, ub);
+    return cudaGetLastError();
+}
+
+cudaError_t launch_explore(int nw, const DevGroup* groups, int ngroups, int ctas, int warps_per_cta, int smem,
+                           unsigned long long budget_ns, int max_rounds, int select_budget, cudaStream_t st)
+{
+    if (nw == 1) {
+        cudaFuncSetAttribute(pbb_explore_kernel<1>, cudaFuncAttributeMaxDynamicSharedMemorySize, smem);
+        pbb_explore_kernel<1><<<ctas, 32 * warps_per_cta, smem, st>>>(groups, ngroups, warps_per_cta, budget_ns,
+                                                                       max_rounds, select_budget);
+    } else {
+        cudaFuncSetAttribute(pbb_explore_kernel<2>, cudaFuncAttributeMaxDynamicSharedMemorySize, smem);
+        pbb_explore_kernel<2><<<ctas, 32 * warps_per_cta, smem, st>>>(groups, ngroups, warps_per_cta, budget_ns,
+                                                                       max_rounds, select_budget);
+    }
+    return cudaGetLastError();
+}
+
+cudaError_t launch_requeue(const DevGroup* groups, int ngroups, cudaStream_t st)
+{
+    dim3 grid(64, ngroups < 65535 ? ngroups : 65535);
+    pbb_requeue_kernel<<<grid, 256, 0, st>>>(groups, ngroups);
+    return cudaGetLastError();
+}
+
+cudaError_t launch_bound(int nw, const DevInstance& I, int count, const int* sched, const int* l1, const int* l2,
+                         int* wb, int* we, int* sb, int* se, int* nweak, int* nstrong, unsigned int* status,
+                         int ctas, int warps_per_cta, int smem, cudaStream_t st)
+{
+    if (nw == 1) {
+        cudaFuncSetAttribute(pbb_bound_kernel<1>, cudaFuncAttributeMaxDynamicSharedMemorySize, smem);
+        pbb_bound_kernel<1><<<ctas, 32 * warps_per_cta, smem, st>>>(I, count, sched, l1, l2, wb, we, sb, se, nweak,
+                                                                     nstrong, status, warps_per_cta);
+    } else {
+        cudaFuncSetAttribute(pbb_bound_kernel<2>, cudaFuncAttributeMaxDynamicSharedMemorySize, smem);
+        pbb_bound_kernel<2><<<ctas, 32 * warps_per_cta, smem, st>>>(I, count, sched, l1, l2, wb, we, sb, se, nweak,
+                                                                     nstrong, status, warps_per_cta);
+    }
+    return cudaGetLastError();
+}
+
+}  // namespace pbbl

@@ -1,0 +1,111 @@
+// Shared host/device definitions of the IVM flow-shop engine.
+#pragma once
+#include <stdint.h>
+
+#define PBB_MAX_N 64          // jobs per instance (int8 IVM cells, two 32-bit mask words)
+#define PBB_MAX_M 32          // machines per instance (one machine per lane in recurrences)
+#define PBB_WARPS_MAX 24
+
+// IVM life cycle (per explorer, in global memory)
+#define IVM_IDLE 0            // no interval
+#define IVM_QUEUED 1          // registered in the idle queue, waiting for a donor
+#define IVM_ACTIVE 2          // holds a non-empty interval
+
+// status bits written by kernels (never traps)
+#define PBB_ST_BADINPUT 1u
+#define PBB_ST_QUEUE 2u
+#define PBB_ST_SPIN 4u
+
+// Packed Johnson entry for (pair i, Johnson position t):
+//   bits 0..7  job id, 8..23 p[m0][job], 24..39 p[m1][job], 40..63 lag[i][job]
+#define JE_JOB(e) ((int)((e) & 0xFFull))
+#define JE_A(e) ((int)(((e) >> 8) & 0xFFFFull))
+#define JE_B(e) ((int)(((e) >> 24) & 0xFFFFull))
+#define JE_C(e) ((int)((e) >> 40))
+
+// One flow-shop instance as the kernels see it (device pointers).
+struct DevInstance {
+    int n, m;
+    int P;        // machine pairs used by the Johnson bound
+    int Ppad;     // P rounded up to 32
+    const int* p;                    // [m][n]
+    const unsigned long long* je;    // [n][Ppad]
+    const unsigned char* pm0;        // [Ppad]
+    const unsigned char* pm1;        // [Ppad]
+    const int* min_arr;              // [m]
+    const int* min_dep;              // [m]
+};
+
+// Search settings shared by a group of explorers.
+struct DevSearch {
+    int bound_mode;    // 0 weak, 1 strong, 2 weak then strong
+    int branch_mode;   // -3,-2,-1 fixed; 1 MaxSum, 2 MinBranch, 3 MinMin
+    int find_all;
+};
+
+// Per-group control block (device memory).
+struct GroupCtl {
+    unsigned long long best_key;   // (cost << 32) | ivm id of the slot holding the permutation
+    int active;                    // explorers holding work
+    int found;                     // leaves that improved (or matched, with findAll) the bound
+    unsigned int status;           // PBB_ST_* bits
+    int pad;
+    unsigned long long decomposed, johnson_bounds, simple_bounds, leaves, root_simple;
+    unsigned long long q_head, q_tail;   // idle-explorer queue cursors
+    unsigned long long steals;           // intervals handed over
+    // work of the Johnson sweeps: nodes swept, free jobs summed over them,
+    // children evaluated by them (roofline accounting)
+    unsigned long long jsweeps, jfree, jchild;
+};
+
+// Explorer storage of a group (device memory, structure of arrays).
+struct DevIvms {
+    int count;             // explorers in the group
+    int npad;              // row stride (64)
+    signed char* mat;      // [count][npad][npad]
+    signed char* pos;      // [count][npad]
+    signed char* end;      // [count][npad]
+    signed char* dir;      // [count][npad]
+    signed char* pj;       // [count][npad] job fixed at each level of the current path
+    int* line;             // [count]
+    int* state;            // [count]
+    int* bestcost;         // [count]
+    signed char* bestperm; // [count][npad]
+    unsigned int* qseq;    // [count] Vyukov queue cell sequence numbers
+    int* qval;             // [count] queued explorer ids
+};
+
+struct DevGroup {
+    DevInstance inst;
+    DevSearch search;
+    DevIvms ivm;
+    GroupCtl* ctl;
+    int first_cta;         // CTAs [first_cta, first_cta + ctas) work on this group
+    int ctas;
+};
+
+// Dynamic shared memory layout of one CTA (host and device agree).
+struct SmemPlan {
+    int je_off, p_off, pm0_off, pm1_off, marr_off, mdep_off, warp_off, warp_bytes, total;
+};
+
+__host__ __device__ inline int pbb_align(int x, int a) { return (x + a - 1) / a * a; }
+
+// per-warp scratch: ints lbF[64] lbB[64] frontZ backZ Fb Bb rem RB FR [32 each];
+// shorts dF[64*m] dB[64*m]; bytes fjob[64] bjob[64] row[64]
+__host__ __device__ inline SmemPlan pbb_smem_plan(int n, int m, int Ppad, int warps)
+{
+    SmemPlan s;
+    int off = 0;
+    s.je_off = off;   off += n * Ppad * 8;
+    s.p_off = off;    off += pbb_align(m * n * 4, 16);
+    s.pm0_off = off;  off += pbb_align(Ppad, 16);
+    s.pm1_off = off;  off += pbb_align(Ppad, 16);
+    s.marr_off = off; off += pbb_align(m * 4, 16);
+    s.mdep_off = off; off += pbb_align(m * 4, 16);
+    s.warp_off = off;
+    s.warp_bytes = pbb_align((2 * PBB_MAX_N + 7 * 32) * 4 + 2 * PBB_MAX_N * m * 2 + 3 * PBB_MAX_N, 16);
+    off += s.warp_bytes * warps;
+    s.total = off;
+    return s;
+}

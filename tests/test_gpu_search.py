@@ -1,0 +1,124 @@
+"""The persistent IVM explorer against the reference: exact node counters at
+UB = optimum, exact optima re-verified from the returned permutation."""
+import numpy as np
+import pytest
+
+from conftest import CONFIG2
+from oracle import Oracle
+import pbbperm_b200 as pb
+from pbbperm_b200.instances import synthetic_instance
+
+pytestmark = pytest.mark.gpu
+
+KEYS = ("decomposed", "johnson_bounds", "simple_bounds", "leaves")
+
+
+def solve(p, ub, ivms=1024, **cfg):
+    with pb.Engine(p, pb.Config(nbIVMs=ivms, **cfg)) as e:
+        return e.solve(ub=ub)
+
+
+def test_counters_vs_reference_golden(search_golden):
+    for r in search_golden["runs"]:
+        if r.get("ub") is None or r.get("big"):
+            continue
+        p = synthetic_instance(r["seed"], r["n"], r["m"])
+        got = solve(p, r["ub"], boundingMode=r["bounding_mode"], adaptiveBranchingMode=r["branching_mode"],
+                    findAll=r["find_all"])
+        assert got["complete"]
+        for k in KEYS:
+            assert got[k] == r[k], (r, k, got[k])
+
+
+@pytest.mark.parametrize("n,m,seed,mode", [(10, 5, 21, 2), (12, 10, 22, 1), (14, 5, 23, 0), (13, 20, 24, 2),
+                                           (35, 10, 45, 0), (35, 10, 45, 2), (2, 3, 33, 2), (3, 2, 34, 1),
+                                           (9, 32, 35, 2), (16, 8, 25, 2)])
+def test_counters_vs_oracle(n, m, seed, mode):
+    p = synthetic_instance(seed, n, m)
+    O = Oracle(p)
+    opt = O.solve(2**31 - 1, bound_mode=2)["best"]
+    want = O.solve(opt, bound_mode=mode)
+    got = solve(p, opt, boundingMode=mode)
+    for k in KEYS:
+        assert got[k] == want[k], (k, got[k], want[k])
+
+
+@pytest.mark.parametrize("mode", [0, 2])
+def test_counters_50x20_below_optimum(mode):
+    """50x20 seed 2 with UB = 3780 (no schedule reaches it, so the search is
+    deterministic): two-word IVM rows, 65536 explorers."""
+    p = synthetic_instance(2, 50, 20)
+    want = Oracle(p).solve(3780, bound_mode=mode)
+    assert want["complete"] and not want["found"]
+    got = solve(p, 3780, ivms=65536, boundingMode=mode)
+    assert got["complete"] and not got["found"]
+    for k in KEYS:
+        assert got[k] == want[k], (k, got[k], want[k])
+
+
+@pytest.mark.parametrize("ivms", [1, 3, 64, 4096, 65536])
+def test_counters_independent_of_explorer_count(ivms):
+    p = synthetic_instance(24, 13, 20)
+    O = Oracle(p)
+    opt = 1803
+    want = O.solve(opt, bound_mode=2)
+    got = solve(p, opt, ivms=ivms, boundingMode=2)
+    for k in KEYS:
+        assert got[k] == want[k], (ivms, k, got[k], want[k])
+
+
+def test_windowed_exploration_matches_single_solve():
+    p = synthetic_instance(24, 13, 20)
+    want = Oracle(p).solve(1803, bound_mode=2)
+    with pb.Engine(p, pb.Config(nbIVMs=2048, boundingMode=2)) as e:
+        e.start(ub=1803)
+        done = False
+        windows = 0
+        while not done and windows < 10000:
+            done = e.explore(0.002)
+            windows += 1
+        got = e.result()
+    assert got["complete"]
+    for k in KEYS:
+        assert got[k] == want[k], (k, got[k], want[k])
+
+
+def test_weak_bound_optimum_ub_inf(search_golden):
+    """20x5 seed 0, weak bound, UB = +inf: optimum equals the reference's and
+    is re-verified from the returned permutation."""
+    ref = [r for r in search_golden["runs"] if r.get("ub") is None][0]
+    p = synthetic_instance(ref["seed"], ref["n"], ref["m"])
+    got = solve(p, pb.INF, ivms=4096, boundingMode=0)
+    assert got["complete"] and got["found"]
+    assert got["cost"] == ref["opt"]
+    assert Oracle(p).eval(got["perm"]) == ref["opt"]
+    assert sorted(got["perm"].tolist()) == list(range(ref["n"]))
+
+
+def test_optimum_found_from_ub_plus_one():
+    p = synthetic_instance(22, 12, 10)
+    got = solve(p, 1012, boundingMode=2)
+    assert got["found"] and got["cost"] == 1011
+    assert Oracle(p).eval(got["perm"]) == 1011
+
+
+def test_root_permutation_respected():
+    p = synthetic_instance(23, 14, 5)
+    O = Oracle(p)
+    root = np.random.default_rng(4).permutation(14).astype(np.int32)
+    want = O.solve(862, bound_mode=2, root=root)
+    with pb.Engine(p, pb.Config(nbIVMs=256, boundingMode=2)) as e:
+        got = e.solve(ub=862, root=root)
+    for k in KEYS:
+        assert got[k] == want[k]
+
+
+def test_config2_20x20_johnson_ub_opt():
+    """20 jobs x 20 machines (seed 1), weak+Johnson bound, 16384 explorers,
+    UB = optimum 2352: decomposed-node count equals the reference's."""
+    c = CONFIG2
+    p = synthetic_instance(c["seed"], c["n"], c["m"])
+    got = solve(p, c["opt"], ivms=16384, boundingMode=2)
+    assert got["complete"]
+    for k in KEYS:
+        assert got[k] == c[k], (k, got[k], c[k])
