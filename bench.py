@@ -231,7 +231,9 @@ def run_ours(args):
     out = None
     if rank == 0:
         # e2e through the C ABI from host buffers (rank 0 measures; all ranks would do the same work)
-        e2e_vals = []
+        e2e_vals = [0.0]
+        if args.e2e_steps > 0:
+            e2e_vals = []
         for _ in range(args.e2e_steps):
             t0 = time.perf_counter()
             with pb.Engine(p, cfg) as e2:
@@ -252,7 +254,7 @@ def run_ours(args):
                     "peak_source": "measured: pbb_diag_int32_peak (IADD+IMNMX register chains, all SMs)",
                     "work_model": kern["work_model"]}
         cpu = None
-        if ws == 1:
+        if ws == 1 and args.cpu_sample > 0:
             r = reference_cpu_run(p, ub, args.cpu_sample)
             if r:
                 cpu = {"value": round(r[0], 1), "unit": "nodes/s", "cores": host_cores(), "kind": "reference",
