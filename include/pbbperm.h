@@ -124,6 +124,23 @@ int pbb_bound_children(const pbb_instance* inst, int32_t johnson_mode, int32_t d
                        int32_t* weak_begin, int32_t* weak_end, int32_t* strong_begin, int32_t* strong_end,
                        int32_t* node_weak, int32_t* node_strong);
 
+/* pbb_bound_children for callers that cannot allocate GPU memory (a plugin
+ * handed only device buffers, code running inside another framework's memory
+ * pool).  No counterpart in the reference.  All node arrays are DEVICE
+ * pointers owned by the caller; `stream` is a cudaStream_t (NULL = default
+ * stream).  The only scratch (the instance tables and a status word) is a
+ * 112 KiB static device array that every GPU loading the library keeps until
+ * exit, so instances are limited to 64 jobs and 20 machines (larger ones:
+ * PBB_E_INVAL).  The first call on a device looks the array up with
+ * cudaGetSymbolAddress -- make it before any stream capture.  Calls share the
+ * array: calls that overlap on the GPU race, so do not issue them
+ * concurrently (the function serialises its own host callers and waits for
+ * `stream` before returning).  Outputs as pbb_bound_children; all required. */
+int pbb_bound_children_noalloc(const pbb_instance* inst, int32_t johnson_mode, int32_t device, void* stream,
+                               int32_t count, const int32_t* sched, const int32_t* limit1, const int32_t* limit2,
+                               int32_t* weak_begin, int32_t* weak_end, int32_t* strong_begin, int32_t* strong_end,
+                               int32_t* node_weak, int32_t* node_strong);
+
 /* NEH upper bound: jobs by decreasing total time, each inserted at the first
  * position of least partial makespan (host code). */
 int pbb_neh(const pbb_instance* inst, int32_t* perm, int32_t* cost);

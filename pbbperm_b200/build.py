@@ -16,7 +16,7 @@ CLI = os.path.join(PKG, "bb")
 ARCH = ["-gencode", "arch=compute_100a,code=sm_100a"]
 NVFLAGS = ARCH + ["-lineinfo", "-O3", "-std=c++17", "-Xcompiler", "-fPIC"]
 
-LIB_SOURCES = ["pbb_kernels.cu", "pbb_host.cu", "pbb_diag.cu"]
+LIB_SOURCES = ["pbb_kernels.cu", "pbb_host.cu", "pbb_diag.cu", "pbb_noalloc.cu"]
 LIB_DEPS = LIB_SOURCES + ["pbb_types.h", "pbb_device.cuh", "pbb_launch.h"]
 HEADERS = ["pbbperm.h", "pbbperm_diag.h"]
 

@@ -215,6 +215,11 @@ int pick_warps(const HostTables& H, int requested, int dev, int& smem)
 
 }  // namespace
 
+namespace pbbh {
+// error message for entry points compiled in other files of the library
+void set_error(const char* msg) { g_err = msg; }
+}  // namespace pbbh
+
 // ---------------------------------------------------------------------------
 // engine
 // ---------------------------------------------------------------------------
