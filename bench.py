@@ -154,6 +154,15 @@ def rank_slice(n, rank, world):
     return pos, end
 
 
+def exchange_incumbent(dist, cost, device):
+    """The ranks' only exchange: the best makespan known anywhere (4-byte
+    MIN all-reduce; NCCL on GPUs, gloo in the CPU tests)."""
+    import torch
+    t = torch.tensor([int(cost)], dtype=torch.int32, device=device)
+    dist.all_reduce(t, op=dist.ReduceOp.MIN)
+    return int(t.item())
+
+
 def run_ours(args):
     import numpy as np
     import torch
@@ -185,9 +194,7 @@ def run_ours(args):
     def exchange_ub(res):
         if dist is None:
             return
-        t = torch.tensor([res["cost"]], dtype=torch.int32, device="cuda")
-        dist.all_reduce(t, op=dist.ReduceOp.MIN)
-        eng.set_ub(int(t.item()))
+        eng.set_ub(exchange_incumbent(dist, res["cost"], "cuda"))
 
     for _ in range(args.warmup):
         _, _, _, res = window()

@@ -64,6 +64,8 @@ def lib():
         L.orc_min_times.argtypes = [ctypes.c_void_p, _i32p, _i32p]
         L.orc_solve.argtypes = [ctypes.c_void_p, ctypes.POINTER(_OrcCfg), ctypes.c_int, _i32p,
                                 ctypes.POINTER(_OrcResult), _i32p]
+        L.orc_solve_interval.argtypes = [ctypes.c_void_p, ctypes.POINTER(_OrcCfg), ctypes.c_int, _i32p, _i32p,
+                                         _i32p, ctypes.POINTER(_OrcResult), _i32p]
         L.orc_neh.argtypes = [ctypes.c_void_p, _i32p]
         L.orc_synthetic_instance.argtypes = [ctypes.c_uint64, ctypes.c_int, ctypes.c_int, ctypes.c_int,
                                              ctypes.c_int, _i32p]
@@ -155,12 +157,16 @@ class Oracle:
         c = lib().orc_neh(self._h, _ptr(perm))
         return c, perm
 
-    def solve(self, ub, bound_mode=2, branch_mode=3, find_all=False, root=None, node_limit=0):
+    def solve(self, ub, bound_mode=2, branch_mode=3, find_all=False, root=None, node_limit=0, pos=None, end=None):
         cfg = _OrcCfg(bound_mode, branch_mode, 1 if find_all else 0, node_limit)
         res = _OrcResult()
         root = np.arange(self.n, dtype=np.int32) if root is None else np.ascontiguousarray(root, dtype=np.int32)
         perm = np.zeros(self.n, np.int32)
-        rc = lib().orc_solve(self._h, ctypes.byref(cfg), int(ub), _ptr(root), ctypes.byref(res), _ptr(perm))
+        pos = None if pos is None else np.ascontiguousarray(pos, dtype=np.int32)
+        end = None if end is None else np.ascontiguousarray(end, dtype=np.int32)
+        rc = lib().orc_solve_interval(self._h, ctypes.byref(cfg), int(ub), _ptr(root), _ptr(pos) if pos is not None
+                                      else None, _ptr(end) if end is not None else None, ctypes.byref(res),
+                                      _ptr(perm))
         if rc != 0:
             raise RuntimeError("oracle solve failed")
         return dict(decomposed=res.decomposed, johnson_bounds=res.johnson_bounds,

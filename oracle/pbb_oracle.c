@@ -611,10 +611,12 @@ static int bb_next(orc_bb *B)
     return 0;
 }
 
-/* Solve from the root row `root` (sequentialbb::setRoot :28-46 -> boundRoot,
- * weak and uncounted; initFullInterval :67-80 -> initAtInterval :84-106 ->
- * unfold) and run next() until the interval is exhausted or node_limit. */
-int orc_solve(const orc_inst *I, const orc_cfg *cfg, int ub, const int *root, orc_result *out, int *best_perm)
+/* Solve the interval [pos, end] (NULL = the whole space) from the root row
+ * `root`: sequentialbb::setRoot :28-46 -> boundRoot (weak, uncounted), then
+ * initAtInterval :84-106 (stats reset, unfold :207-264), then next() until
+ * the interval is exhausted or node_limit. */
+int orc_solve_interval(const orc_inst *I, const orc_cfg *cfg, int ub, const int *root, const int *pos,
+                       const int *end, orc_result *out, int *best_perm)
 {
     int n = I->n;
     orc_bb B;
@@ -630,7 +632,11 @@ int orc_solve(const orc_inst *I, const orc_cfg *cfg, int ub, const int *root, or
     B.dir[0] = choose_dir(&B, B.cb_w, B.ce_w);
     prune(&B, B.cb_w, B.ce_w, B.cb_w, B.ce_w);
     memset(&B.res, 0, sizeof(B.res));                     /* initAtInterval resets the stats */
-    for (int i = 0; i < n; i++) { B.pos[i] = 0; B.end[i] = n - i - 1; }
+    for (int i = 0; i < n; i++) {
+        B.pos[i] = pos ? pos[i] : 0;
+        B.end[i] = end ? end[i] : n - i - 1;
+        if (B.pos[i] < 0 || B.pos[i] >= n - i || B.end[i] < 0 || B.end[i] >= n - i) { free(B.mat); return -2; }
+    }
     if (before_end(&B)) unfold(&B);
     int complete = 1;
     while (bb_next(&B)) {
@@ -641,6 +647,11 @@ int orc_solve(const orc_inst *I, const orc_cfg *cfg, int ub, const int *root, or
     *out = B.res;
     free(B.mat);
     return 0;
+}
+
+int orc_solve(const orc_inst *I, const orc_cfg *cfg, int ub, const int *root, orc_result *out, int *best_perm)
+{
+    return orc_solve_interval(I, cfg, ub, root, NULL, NULL, out, best_perm);
 }
 
 /* ------------------------------------------------------------------------ */

@@ -122,3 +122,30 @@ def test_config2_20x20_johnson_ub_opt():
     assert got["complete"]
     for k in KEYS:
         assert got[k] == c[k], (k, got[k], c[k])
+
+
+@pytest.mark.parametrize("world", [2, 3])
+def test_interval_start_matches_oracle(world):
+    """pbb_start_interval (gpubb::initAtInterval) on each rank's root slice:
+    per-slice counters equal the oracle's interval solve, and the best of the
+    slices is the optimum."""
+    import bench
+    p = synthetic_instance(24, 13, 20)
+    O = Oracle(p)
+    found = []
+    for r in range(world):
+        pos, end = bench.rank_slice(13, r, world)
+        want = O.solve(1804, bound_mode=2, pos=pos, end=end)
+        with pb.Engine(p, pb.Config(nbIVMs=1024, boundingMode=2)) as e:
+            e.start_interval(ub=1804, pos=pos, end=end)
+            while not e.explore(1.0):
+                pass
+            got = e.result()
+        assert got["complete"]
+        if want["found"]:
+            assert got["found"] and got["cost"] == want["best"]
+            found.append(got["cost"])
+        else:
+            for k in KEYS:
+                assert got[k] == want[k], (r, k, got[k], want[k])
+    assert min(found) == 1803
