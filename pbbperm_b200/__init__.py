@@ -69,7 +69,8 @@ class _Work(ctypes.Structure):
                 ("machine_pairs", ctypes.c_int32), ("explorers", ctypes.c_int32), ("warps", ctypes.c_int32),
                 ("pad", ctypes.c_int32), ("decomposed", ctypes.c_uint64), ("simple_bounds", ctypes.c_uint64),
                 ("johnson_bounds", ctypes.c_uint64), ("johnson_sweeps", ctypes.c_uint64),
-                ("sweep_free_jobs", ctypes.c_uint64), ("sweep_children", ctypes.c_uint64)]
+                ("sweep_free_jobs", ctypes.c_uint64), ("sweep_children", ctypes.c_uint64),
+                ("direct_children", ctypes.c_uint64), ("direct_free_jobs", ctypes.c_uint64)]
 
 
 _lib = None
@@ -97,6 +98,9 @@ def lib():
         L.pbb_start_interval.argtypes = [ctypes.c_void_p, ctypes.c_int32, _i32p, _i32p, _i32p]
         L.pbb_set_ub.argtypes = [ctypes.c_void_p, ctypes.c_int32]
         L.pbb_work_counters.argtypes = [ctypes.c_void_p, ctypes.POINTER(_Work)]
+        L.pbb_diag_bound_children.argtypes = [ctypes.POINTER(_Instance), ctypes.c_int32, ctypes.c_int32,
+                                               ctypes.c_int32, ctypes.c_int32, _i32p, _i32p, _i32p, _i32p, _i32p,
+                                               _i32p, _i32p, _i32p, _i32p]
         L.pbb_diag_int32_peak.argtypes = [ctypes.c_int32, ctypes.POINTER(ctypes.c_double),
                                           ctypes.POINTER(ctypes.c_double)]
         _lib = L
@@ -202,17 +206,22 @@ class Engine:
         """Work of the explorer kernels since start, with the INT32 op model
         of the bounds: weak child 5m ops (add/max chain per machine); per
         Johnson sweep and machine pair, 2 membership tests per position and
-        pass, 5 ops per free job and pass, 9 ops per evaluated child."""
+        pass, 5 ops per free job and pass, 9 ops per evaluated child; per
+        directly scanned child and pair, 1 test per position and 4 ops per
+        free job."""
         w = _Work()
         _check(lib().pbb_work_counters(self._h, ctypes.byref(w)))
         m, n, P = w.n_machines, w.n_jobs, w.machine_pairs
         ops = (5 * m * w.simple_bounds +
-               P * (4 * n * w.johnson_sweeps + 10 * w.sweep_free_jobs + 9 * w.sweep_children))
+               P * (4 * n * w.johnson_sweeps + 10 * w.sweep_free_jobs + 9 * w.sweep_children) +
+               P * (n * w.direct_children + 4 * w.direct_free_jobs))
         return dict(device_seconds=w.device_seconds, int32_ops=float(ops), decomposed=w.decomposed,
                     simple_bounds=w.simple_bounds, johnson_bounds=w.johnson_bounds,
                     johnson_sweeps=w.johnson_sweeps, sweep_free_jobs=w.sweep_free_jobs,
-                    sweep_children=w.sweep_children, explorers=w.explorers, warps=w.warps,
-                    work_model="5m per weak child + P*(4n per sweep + 10 per free job + 9 per child)")
+                    sweep_children=w.sweep_children, direct_children=w.direct_children,
+                    explorers=w.explorers, warps=w.warps,
+                    work_model="5m per weak child + P*(4n per sweep + 10 per swept free job + 9 per swept child)"
+                               " + P*(n + 4 per free job) per directly scanned child")
 
     def explore(self, seconds):
         done = ctypes.c_int32(0)
@@ -225,12 +234,13 @@ class Engine:
         return _result(r)
 
 
-def bound_children(p, sched, limit1, limit2, johnson_mode=0, device=0):
+def bound_children(p, sched, limit1, limit2, johnson_mode=0, device=0, method=None):
     """Children LBs of a batch of nodes on the GPU.
 
     Returns dict of (count x n) arrays weak_begin, weak_end, strong_begin,
     strong_end (by job id, 0 for fixed jobs) and (count,) node_weak,
-    node_strong."""
+    node_strong.  method (diagnostic): 0 = sweeps, 1 = direct per-child
+    scans; None = the default entry point."""
     inst, p = _instance(p)
     n = p.shape[1]
     sched = np.ascontiguousarray(sched, dtype=np.int32).reshape(-1, n)
@@ -240,9 +250,14 @@ def bound_children(p, sched, limit1, limit2, johnson_mode=0, device=0):
     out = {k: np.zeros((cnt, n), np.int32) for k in ("weak_begin", "weak_end", "strong_begin", "strong_end")}
     out["node_weak"] = np.zeros(cnt, np.int32)
     out["node_strong"] = np.zeros(cnt, np.int32)
-    _check(lib().pbb_bound_children(ctypes.byref(inst), johnson_mode, device, cnt, _ptr(sched), _ptr(l1), _ptr(l2),
-                                    _ptr(out["weak_begin"]), _ptr(out["weak_end"]), _ptr(out["strong_begin"]),
-                                    _ptr(out["strong_end"]), _ptr(out["node_weak"]), _ptr(out["node_strong"])))
+    outs = (_ptr(out["weak_begin"]), _ptr(out["weak_end"]), _ptr(out["strong_begin"]), _ptr(out["strong_end"]),
+            _ptr(out["node_weak"]), _ptr(out["node_strong"]))
+    if method is None:
+        _check(lib().pbb_bound_children(ctypes.byref(inst), johnson_mode, device, cnt, _ptr(sched), _ptr(l1), _ptr(l2),
+                                        *outs))
+    else:
+        _check(lib().pbb_diag_bound_children(ctypes.byref(inst), johnson_mode, device, method, cnt, _ptr(sched),
+                                             _ptr(l1), _ptr(l2), *outs))
     return out
 
 

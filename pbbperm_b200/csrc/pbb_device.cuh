@@ -14,6 +14,8 @@
 
 #define FULLMASK 0xffffffffu
 #define NEG_INF (-(1 << 28))
+// at most this many children are bounded by direct scans instead of sweeps
+#define PBB_DIRECT_MAX 2
 
 namespace pbb {
 
@@ -100,6 +102,7 @@ struct CtaTables {
     const unsigned char* pm1;
     const int* min_arr;
     const int* min_dep;
+    const unsigned char* posj;     // [n][Ppad] or NULL
     int n, m, P, Ppad;
 };
 
@@ -357,6 +360,188 @@ __device__ __forceinline__ void johnson_children(const CtaTables& T, const WarpS
     __syncwarp();
 }
 
+// Johnson LB of a few children by direct scans (bound_fsp_strong.cpp:76-100
+// run per child): lanes own (machine pair, child) combinations, each scans the
+// pair's Johnson order over the free jobs minus the child's own job, with the
+// recurrence predicated instead of branched, and merges its pair maximum with
+// one shared-memory atomicMax.  Cheaper than the two sweeps of
+// johnson_children when only one to three children are evaluated.
+// cjob/cside: the children's jobs and sides (0 front, 1 back), nc <= 4.
+template <int NW>
+__device__ __forceinline__ void johnson_direct(const CtaTables& T, const WarpScratch& S, const unsigned (&um)[NW],
+                                               int nc, const int (&cjob)[4], const int (&cside)[4])
+{
+    const int lane = lane_id();
+    const int n = T.n, m = T.m, P = T.P;
+    const unsigned long long free_all =
+        (NW > 1 ? ((unsigned long long)um[NW > 1 ? 1 : 0] << 32) : 0ull) | (unsigned long long)um[0];
+    const int combos = P * nc;
+    for (int base = 0; base < combos; base += 32) {
+        const int q = base + lane;
+        if (q < combos) {
+            int ci = 0, i = q;
+            while (i >= P) { i -= P; ci++; }
+            int u = cjob[0], side = cside[0];
+#pragma unroll
+            for (int c = 1; c < 4; c++)
+                if (ci == c) { u = cjob[c]; side = cside[c]; }
+            const int m0 = T.pm0[i], m1 = T.pm1[i];
+            int t0, t1, B0, B1;
+            if (side == 0) {
+                t0 = S.frontZ[m0] + S.dF[u * m + m0];
+                t1 = S.frontZ[m1] + S.dF[u * m + m1];
+                B0 = S.Bb[m0];
+                B1 = S.Bb[m1];
+            } else {
+                t0 = S.Fb[m0];
+                t1 = S.Fb[m1];
+                B0 = S.backZ[m0] + S.dB[u * m + m0];
+                B1 = S.backZ[m1] + S.dB[u * m + m1];
+            }
+            const unsigned long long fm = free_all & ~(1ull << u);
+            const unsigned long long* col = T.je + i;
+#pragma unroll 2
+            for (int t = 0; t < n; t++) {
+                const unsigned long long e = col[t * T.Ppad];
+                const bool fr = (fm >> JE_JOB(e)) & 1ull;
+                const int t0n = t0 + JE_A(e);
+                const int t1n = max(t1, t0n + JE_C(e)) + JE_B(e);
+                t0 = fr ? t0n : t0;
+                t1 = fr ? t1n : t1;
+            }
+            atomicMax(side ? &S.lbB[u] : &S.lbF[u], max(t1 + B1, t0 + B0));
+        }
+    }
+    __syncwarp();
+}
+
+// Johnson positions (for the lane's pair i) holding a free job, as a 64-bit
+// mask built from the inverse Johnson order T.posj: scans then visit only the
+// k free positions instead of all n.
+__device__ __forceinline__ unsigned long long free_positions(const CtaTables& T, const WarpScratch& S, int k, int i)
+{
+    unsigned long long pm = 0ull;
+    const unsigned char* col = T.posj + i;
+    for (int q = 0; q < k; q++) pm |= 1ull << col[S.rowj[q] * T.Ppad];
+    return pm;
+}
+
+// johnson_direct over the free positions only (needs T.posj).
+template <int NW>
+__device__ __forceinline__ void johnson_direct_masked(const CtaTables& T, const WarpScratch& S, int k, int nc,
+                                                      const int (&cjob)[4], const int (&cside)[4])
+{
+    const int lane = lane_id();
+    const int m = T.m, P = T.P;
+    const int combos = P * nc;
+    for (int base = 0; base < combos; base += 32) {
+        const int q = base + lane;
+        if (q < combos) {
+            int ci = 0, i = q;
+            while (i >= P) { i -= P; ci++; }
+            int u = cjob[0], side = cside[0];
+#pragma unroll
+            for (int c = 1; c < 4; c++)
+                if (ci == c) { u = cjob[c]; side = cside[c]; }
+            const int m0 = T.pm0[i], m1 = T.pm1[i];
+            int t0, t1, B0, B1;
+            if (side == 0) {
+                t0 = S.frontZ[m0] + S.dF[u * m + m0];
+                t1 = S.frontZ[m1] + S.dF[u * m + m1];
+                B0 = S.Bb[m0];
+                B1 = S.Bb[m1];
+            } else {
+                t0 = S.Fb[m0];
+                t1 = S.Fb[m1];
+                B0 = S.backZ[m0] + S.dB[u * m + m0];
+                B1 = S.backZ[m1] + S.dB[u * m + m1];
+            }
+            unsigned long long pm = free_positions(T, S, k, i) & ~(1ull << T.posj[u * T.Ppad + i]);
+            const unsigned long long* col = T.je + i;
+            while (pm) {
+                const int t = __ffsll((long long)pm) - 1;
+                pm &= pm - 1ull;
+                const unsigned long long e = col[t * T.Ppad];
+                t0 += JE_A(e);
+                t1 = max(t1, t0 + JE_C(e)) + JE_B(e);
+            }
+            atomicMax(side ? &S.lbB[u] : &S.lbF[u], max(t1 + B1, t0 + B0));
+        }
+    }
+    __syncwarp();
+}
+
+// johnson_children (forward + backward max-plus sweeps) over the free
+// positions only (needs T.posj); same results, O(P k) instead of O(P n).
+template <int NW>
+__device__ __forceinline__ void johnson_sweep_masked(const CtaTables& T, const WarpScratch& S, int k, bool doF,
+                                                     const unsigned (&sF)[NW], bool doB, const unsigned (&sB)[NW])
+{
+    const int lane = lane_id();
+    const int m = T.m;
+    for (int base = 0; base < T.P; base += 32) {
+        const int i = base + lane;
+        if (i < T.P) {
+            const int m0 = T.pm0[i], m1 = T.pm1[i];
+            const int Asum = S.rem[m0], Bsum = S.rem[m1];
+            const int cF1 = S.frontZ[m1] + Bsum + S.Bb[m1];
+            const int cF2 = S.frontZ[m0] + S.Bb[m1];
+            const int cF3 = S.frontZ[m0] + Asum + S.Bb[m0];
+            const int cB1 = S.Fb[m1] + Bsum + S.backZ[m1];
+            const int cB2 = S.Fb[m0] + S.backZ[m1];
+            const int cB3 = S.Fb[m0] + Asum + S.backZ[m0];
+            const unsigned long long* col = T.je + i;
+            const unsigned long long pm = free_positions(T, S, k, i);
+            int Apre = 0, Bpre = 0, PMx = NEG_INF;
+            unsigned long long f = pm;
+            while (f) {
+                const int t = __ffsll((long long)f) - 1;
+                f &= f - 1ull;
+                const unsigned long long e = col[t * T.Ppad];
+                const int u = JE_JOB(e);
+                const unsigned bit = 1u << (u & 31);
+                unsigned fw = sF[0], bw = sB[0];
+#pragma unroll
+                for (int w = 1; w < NW; w++)
+                    if ((u >> 5) == w) { fw = sF[w]; bw = sB[w]; }
+                const int a = JE_A(e), b = JE_B(e), c = JE_C(e);
+                Apre += a;
+                const int W = Apre - Bpre + c + Bsum;
+                if (doF && (fw & bit)) {
+                    const int d0 = S.dF[u * m + m0], d1 = S.dF[u * m + m1];
+                    atomicMax(&S.lbF[u], max(max(cF1 + d1 - b, cF2 + d0 + PMx - b), cF3 + d0 - a));
+                }
+                if (doB && (bw & bit)) {
+                    const int d0 = S.dB[u * m + m0], d1 = S.dB[u * m + m1];
+                    atomicMax(&S.lbB[u], max(max(cB1 - b, cB2 + PMx - b) + d1, cB3 - a + d0));
+                }
+                PMx = max(PMx, W);
+                Bpre += b;
+            }
+            int Asuf = 0, Bsuf = 0, SMx = NEG_INF;
+            unsigned long long r = pm;
+            while (r) {
+                const int t = 63 - __clzll((long long)r);
+                r &= ~(1ull << t);
+                const unsigned long long e = col[t * T.Ppad];
+                const int u = JE_JOB(e);
+                const unsigned bit = 1u << (u & 31);
+                unsigned fw = sF[0], bw = sB[0];
+#pragma unroll
+                for (int w = 1; w < NW; w++)
+                    if ((u >> 5) == w) { fw = sF[w]; bw = sB[w]; }
+                const int a = JE_A(e), b = JE_B(e), c = JE_C(e);
+                if (doF && (fw & bit)) atomicMax(&S.lbF[u], cF2 + S.dF[u * m + m0] + SMx - a);
+                if (doB && (bw & bit)) atomicMax(&S.lbB[u], cB2 + SMx - a + S.dB[u * m + m1]);
+                Bsuf += b;
+                SMx = max(SMx, Asum - Asuf + c + Bsuf);
+                Asuf += a;
+            }
+        }
+    }
+    __syncwarp();
+}
+
 // Per-child head/tail deltas used by johnson_children (front child u: heads of
 // front + u; back child u: tails of u + back).  Lane per free cell.
 template <int NW>
@@ -470,7 +655,7 @@ __device__ __forceinline__ int choose_dir(int rule, int line, int ub, const int 
 
 struct NodeCounters {
     unsigned long long simple, johnson;
-    unsigned long long sweeps, free_jobs, swept_children;
+    unsigned long long sweeps, free_jobs, swept_children, direct_children, direct_free;
 };
 
 // Bound the children of the node whose free jobs are `row[0..k)` (front and
@@ -553,10 +738,36 @@ __device__ __forceinline__ int bound_and_prune(const CtaTables& T, const WarpScr
                     if (w * 32 + lane < PBB_MAX_N) { S.lbF[w * 32 + lane] = 0; S.lbB[w * 32 + lane] = 0; }
                 }
                 child_tables<NW>(T, S, row, k, nF > 0, sF, nB > 0, sB);
-                johnson_children<NW>(T, S, um, nF > 0, sF, nB > 0, sB, nullptr);
-                cnt.sweeps++;
-                cnt.free_jobs += k;
-                cnt.swept_children += nF + nB;
+                if (nF + nB <= PBB_DIRECT_MAX) {
+                    // list the children (front side first, job order)
+                    int cjob[4] = {0, 0, 0, 0}, cside[4] = {0, 0, 0, 0};
+                    int nc = 0;
+#pragma unroll
+                    for (int side = 0; side < 2; side++) {
+#pragma unroll
+                        for (int q = 0; q < NW; q++) {
+                            unsigned msk = side ? sB[q] : sF[q];
+                            while (msk) {
+                                const int j = q * 32 + __ffs(msk) - 1;
+                                msk &= msk - 1;
+#pragma unroll
+                                for (int c = 0; c < 4; c++)
+                                    if (nc == c) { cjob[c] = j; cside[c] = side; }
+                                nc++;
+                            }
+                        }
+                    }
+                    if (T.posj) johnson_direct_masked<NW>(T, S, k, nc, cjob, cside);
+                    else johnson_direct<NW>(T, S, um, nc, cjob, cside);
+                    cnt.direct_children += nc;
+                    cnt.direct_free += (unsigned long long)nc * k;
+                } else {
+                    if (T.posj) johnson_sweep_masked<NW>(T, S, k, nF > 0, sF, nB > 0, sB);
+                    else johnson_children<NW>(T, S, um, nF > 0, sF, nB > 0, sB, nullptr);
+                    cnt.sweeps++;
+                    cnt.free_jobs += k;
+                    cnt.swept_children += nF + nB;
+                }
 #pragma unroll
                 for (int w = 0; w < NW; w++) {
                     if (pF[w]) cbs[w] = S.lbF[row[w]];

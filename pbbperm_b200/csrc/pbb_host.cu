@@ -44,7 +44,7 @@ struct HostTables {
     int n = 0, m = 0, P = 0, Ppad = 0;
     std::vector<int> p, min_arr, min_dep;
     std::vector<unsigned long long> je;
-    std::vector<unsigned char> pm0, pm1;
+    std::vector<unsigned char> pm0, pm1, posj;
 };
 
 // Johnson's rule with the reference's tie order: keys (group, value); group 1
@@ -133,6 +133,7 @@ int build_tables(const pbb_instance* inst, int johnson_mode, HostTables& H)
     H.P = (int)pairs.size();
     H.Ppad = (H.P + 31) / 32 * 32;
     H.je.assign((size_t)n * H.Ppad, 0ull);
+    H.posj.assign((size_t)n * H.Ppad, 0);
     H.pm0.assign(H.Ppad, 0);
     H.pm1.assign(H.Ppad, 0);
     JohnsonKeys K;
@@ -159,6 +160,7 @@ int build_tables(const pbb_instance* inst, int johnson_mode, HostTables& H)
                                          ((unsigned long long)H.p[b * n + j] << 24) |
                                          ((unsigned long long)lag[j] << 40);
             H.je[(size_t)t * H.Ppad + i] = e;
+            H.posj[(size_t)j * H.Ppad + i] = (unsigned char)t;
         }
     }
     return PBB_OK;
@@ -168,6 +170,7 @@ struct DeviceInstance {
     int* p = nullptr;
     unsigned long long* je = nullptr;
     unsigned char* pm = nullptr;
+    unsigned char* posj = nullptr;
     int* mt = nullptr;
     DevInstance view{};
 
@@ -176,22 +179,25 @@ struct DeviceInstance {
         CK(cudaMalloc(&p, sizeof(int) * H.n * H.m));
         CK(cudaMalloc(&je, sizeof(unsigned long long) * H.je.size()));
         CK(cudaMalloc(&pm, 2 * H.Ppad));
+        CK(cudaMalloc(&posj, H.posj.size()));
         CK(cudaMalloc(&mt, sizeof(int) * 2 * H.m));
         CK(cudaMemcpyAsync(p, H.p.data(), sizeof(int) * H.n * H.m, cudaMemcpyHostToDevice, st));
         CK(cudaMemcpyAsync(je, H.je.data(), sizeof(unsigned long long) * H.je.size(), cudaMemcpyHostToDevice, st));
         CK(cudaMemcpyAsync(pm, H.pm0.data(), H.Ppad, cudaMemcpyHostToDevice, st));
+        CK(cudaMemcpyAsync(posj, H.posj.data(), H.posj.size(), cudaMemcpyHostToDevice, st));
         CK(cudaMemcpyAsync(pm + H.Ppad, H.pm1.data(), H.Ppad, cudaMemcpyHostToDevice, st));
         CK(cudaMemcpyAsync(mt, H.min_arr.data(), sizeof(int) * H.m, cudaMemcpyHostToDevice, st));
         CK(cudaMemcpyAsync(mt + H.m, H.min_dep.data(), sizeof(int) * H.m, cudaMemcpyHostToDevice, st));
         view.n = H.n; view.m = H.m; view.P = H.P; view.Ppad = H.Ppad;
         view.p = p; view.je = je; view.pm0 = pm; view.pm1 = pm + H.Ppad;
         view.min_arr = mt; view.min_dep = mt + H.m;
+        view.posj = posj;
         return PBB_OK;
     }
     void release()
     {
-        cudaFree(p); cudaFree(je); cudaFree(pm); cudaFree(mt);
-        p = nullptr; je = nullptr; pm = nullptr; mt = nullptr;
+        cudaFree(p); cudaFree(je); cudaFree(pm); cudaFree(mt); cudaFree(posj);
+        p = nullptr; je = nullptr; pm = nullptr; mt = nullptr; posj = nullptr;
     }
 };
 
@@ -502,10 +508,35 @@ int pbb_solve(pbb_engine* e, int32_t ub, const int32_t* root_perm, double time_l
     return pbb_get_result(e, out);
 }
 
+static int bound_children_impl(const pbb_instance* inst, int32_t johnson_mode, int32_t device, int32_t method,
+                               int32_t count, const int32_t* sched, const int32_t* limit1, const int32_t* limit2,
+                               int32_t* weak_begin, int32_t* weak_end, int32_t* strong_begin, int32_t* strong_end,
+                               int32_t* node_weak, int32_t* node_strong);
+
 int pbb_bound_children(const pbb_instance* inst, int32_t johnson_mode, int32_t device, int32_t count,
                        const int32_t* sched, const int32_t* limit1, const int32_t* limit2, int32_t* weak_begin,
                        int32_t* weak_end, int32_t* strong_begin, int32_t* strong_end, int32_t* node_weak,
                        int32_t* node_strong)
+{
+    return bound_children_impl(inst, johnson_mode, device, 0, count, sched, limit1, limit2, weak_begin, weak_end,
+                               strong_begin, strong_end, node_weak, node_strong);
+}
+
+int pbb_diag_bound_children(const pbb_instance* inst, int32_t johnson_mode, int32_t device, int32_t method,
+                            int32_t count, const int32_t* sched, const int32_t* limit1, const int32_t* limit2,
+                            int32_t* weak_begin, int32_t* weak_end, int32_t* strong_begin, int32_t* strong_end,
+                            int32_t* node_weak, int32_t* node_strong)
+{
+    if (method < 0 || method > 2)
+        return fail(PBB_E_INVAL, "method must be 0 (sweeps), 1 (direct scans) or 2 (sweeps over free positions)");
+    return bound_children_impl(inst, johnson_mode, device, method, count, sched, limit1, limit2, weak_begin,
+                               weak_end, strong_begin, strong_end, node_weak, node_strong);
+}
+
+static int bound_children_impl(const pbb_instance* inst, int32_t johnson_mode, int32_t device, int32_t method,
+                               int32_t count, const int32_t* sched, const int32_t* limit1, const int32_t* limit2,
+                               int32_t* weak_begin, int32_t* weak_end, int32_t* strong_begin, int32_t* strong_end,
+                               int32_t* node_weak, int32_t* node_strong)
 {
     if (count < 0 || (count > 0 && (!sched || !limit1 || !limit2))) return fail(PBB_E_INVAL, "bad node arrays");
     HostTables H;
@@ -557,7 +588,7 @@ int pbb_bound_children(const pbb_instance* inst, int32_t johnson_mode, int32_t d
         int ctas = (count + warps - 1) / warps;
         ctas = std::min(ctas, sms * 4);
         ce = pbbl::launch_bound(n <= 32 ? 1 : 2, di.view, count, d_s, d_l1, d_l2, d_wb, d_we, d_sb, d_se, d_nw, d_ns,
-                                status, ctas, warps, smem, st);
+                                status, ctas, warps, smem, st, method);
         if (ce != cudaSuccess) { rc = cuda_fail(ce, "pbb_bound_kernel launch"); break; }
         if (weak_begin) cudaMemcpyAsync(weak_begin, d_wb, sizeof(int) * cn, cudaMemcpyDeviceToHost, st);
         if (weak_end) cudaMemcpyAsync(weak_end, d_we, sizeof(int) * cn, cudaMemcpyDeviceToHost, st);
@@ -595,6 +626,8 @@ int pbb_work_counters(pbb_engine* e, pbb_work* out)
     out->johnson_sweeps = c.jsweeps;
     out->sweep_free_jobs = c.jfree;
     out->sweep_children = c.jchild;
+    out->direct_children = c.jdirect;
+    out->direct_free_jobs = c.jdirect_free;
     out->explorers = e->cfg.nb_ivms;
     out->warps = e->warps * e->ctas;
     return PBB_OK;

@@ -68,7 +68,11 @@ __device__ void load_tables(const DevInstance& I, unsigned char* smem, const Sme
     for (int i = tid; i < I.n * I.m; i += nt) p[i] = I.p[i];
     for (int i = tid; i < I.Ppad; i += nt) { pm0[i] = I.pm0[i]; pm1[i] = I.pm1[i]; }
     for (int i = tid; i < I.m; i += nt) { marr[i] = I.min_arr[i]; mdep[i] = I.min_dep[i]; }
+    unsigned char* posj = smem + sp.posj_off;
+    if (I.posj)
+        for (int i = tid; i < I.n * I.Ppad; i += nt) posj[i] = I.posj[i];
     T.je = je; T.p = p; T.pm0 = pm0; T.pm1 = pm1; T.min_arr = marr; T.min_dep = mdep;
+    T.posj = I.posj ? posj : nullptr;
     T.n = I.n; T.m = I.m; T.P = I.P; T.Ppad = I.Ppad;
 }
 
@@ -154,14 +158,14 @@ __device__ __forceinline__ void build_lists(const WarpScratch& S, const Ivm<NW>&
 
 struct WarpCounters {
     unsigned long long decomposed, simple, johnson, leaves;
-    unsigned long long sweeps, free_jobs, swept_children;
+    unsigned long long sweeps, free_jobs, swept_children, direct_children, direct_free;
 };
 
 // Record an improving leaf: permutation into the explorer's slot, then the
 // (cost, explorer) key into the group's best (solution.cpp:27-45 restated as
 // a packed atomicMin instead of a mutex).
 template <int NW>
-__device__ void record_solution(const DevGroup& G, const WarpScratch& S, int id, int f, int b, int last, int cost)
+__device__ __forceinline__ void record_solution(const DevGroup& G, const WarpScratch& S, int id, int f, int b, int last, int cost)
 {
     const int n = G.inst.n;
     signed char* slot = G.ivm.bestperm + (size_t)id * G.ivm.npad;
@@ -187,7 +191,7 @@ __device__ void record_solution(const DevGroup& G, const WarpScratch& S, int id,
 // way.  Returns 1 with a node to bound at R.line, 0 when the interval is
 // exhausted, 2 when the selection budget ran out (state stays consistent).
 template <int NW>
-__device__ int select_node(const DevGroup& G, const CtaTables& T, const WarpScratch& S, int id, Ivm<NW>& R,
+__device__ __forceinline__ int select_node(const DevGroup& G, const CtaTables& T, const WarpScratch& S, int id, Ivm<NW>& R,
                            int& best, WarpCounters& C, int budget)
 {
     const int n = T.n;
@@ -285,6 +289,8 @@ __device__ __forceinline__ void bound_current(const DevGroup& G, const CtaTables
     C.sweeps += nc.sweeps;
     C.free_jobs += nc.free_jobs;
     C.swept_children += nc.swept_children;
+    C.direct_children += nc.direct_children;
+    C.direct_free += nc.direct_free;
 }
 
 // ---------------------------------------------------------------------------
@@ -342,7 +348,7 @@ __device__ int queue_pop(const DevGroup& G)
 // without an uncounted unfold, so decomposed-node counts do not depend on
 // how the work was shared.
 template <int NW>
-__device__ void try_share(const DevGroup& G, int id, Ivm<NW>& R)
+__device__ __forceinline__ void try_share(const DevGroup& G, int id, Ivm<NW>& R)
 {
     const int n = G.inst.n;
     // cheap emptiness test of the queue first
@@ -475,6 +481,7 @@ __global__ void pbb_reset_kernel(const DevGroup* groups, int ngroups, const int*
             c->decomposed = c->johnson_bounds = c->simple_bounds = c->leaves = c->root_simple = 0;
             c->q_head = c->q_tail = 0; c->steals = 0;
             c->jsweeps = c->jfree = c->jchild = 0;
+            c->jdirect = c->jdirect_free = 0;
         }
     }
 }
@@ -553,6 +560,8 @@ __global__ void pbb_root_kernel(const DevGroup* groups, int ngroups, const int* 
         G.ctl->jsweeps += nc.sweeps;
         G.ctl->jfree += nc.free_jobs;
         G.ctl->jchild += nc.swept_children;
+        G.ctl->jdirect += nc.direct_children;
+        G.ctl->jdirect_free += nc.direct_free;
         if (alive) {
             G.ctl->active = 1;
             G.ivm.state[id] = IVM_ACTIVE;
@@ -582,7 +591,7 @@ pbb_explore_kernel(const DevGroup* groups, int ngroups, int warps_per_cta, unsig
     const int mode = G.search.bound_mode;
     const unsigned long long t0 = globaltimer_ns();
 
-    WarpCounters C = {0, 0, 0, 0, 0, 0, 0};
+    WarpCounters C = {0, 0, 0, 0, 0, 0, 0, 0, 0};
     Ivm<NW> R;
     int cached = -1;                   // explorer whose state is held in registers
     const bool single = (G.ivm.count <= W);
@@ -638,6 +647,8 @@ pbb_explore_kernel(const DevGroup* groups, int ngroups, int warps_per_cta, unsig
         atomicAdd(&G.ctl->jsweeps, C.sweeps);
         atomicAdd(&G.ctl->jfree, C.free_jobs);
         atomicAdd(&G.ctl->jchild, C.swept_children);
+        atomicAdd(&G.ctl->jdirect, C.direct_children);
+        atomicAdd(&G.ctl->jdirect_free, C.direct_free);
     }
 }
 
@@ -668,7 +679,7 @@ __global__ void pbb_requeue_kernel(const DevGroup* groups, int ngroups)
 template <int NW>
 __global__ void pbb_bound_kernel(DevInstance I, int count, const int* sched, const int* l1s, const int* l2s,
                                  int* wb, int* we, int* sb, int* se, int* node_weak, int* node_strong,
-                                 unsigned int* status, int warps_per_cta)
+                                 unsigned int* status, int warps_per_cta, int method)
 {
     extern __shared__ __align__(16) unsigned char smem[];
     const SmemPlan sp = pbb_smem_plan(I.n, I.m, I.Ppad, warps_per_cta);
@@ -755,8 +766,31 @@ __global__ void pbb_bound_kernel(DevInstance I, int count, const int* sched, con
             for (int q = 0; q < NW; q++) none[q] = 0;
             if (kids) child_tables<NW>(T, S, row, k, true, um, true, um);
             int nl = 0;
-            if (kids) johnson_children<NW>(T, S, um, true, um, true, um, &nl);
-            else johnson_children<NW>(T, S, um, false, none, false, none, &nl);
+            if (kids && method == 0) {
+                johnson_children<NW>(T, S, um, true, um, true, um, &nl);
+            } else if (kids && method == 2 && T.posj) {
+                johnson_children<NW>(T, S, um, false, none, false, none, &nl);
+                johnson_sweep_masked<NW>(T, S, k, true, um, true, um);
+            } else {
+                johnson_children<NW>(T, S, um, false, none, false, none, &nl);
+                if (kids) {
+                    // direct scans, four children at a time (front side, then back side)
+                    int cjob[4] = {0, 0, 0, 0}, cside[4] = {0, 0, 0, 0};
+                    int nc = 0;
+                    for (int c = 0; c < 2 * k; c++) {
+                        const int j = vget<NW>(row, c < k ? c : c - k);
+#pragma unroll
+                        for (int q = 0; q < 4; q++)
+                            if (nc == q) { cjob[q] = j; cside[q] = c < k ? 0 : 1; }
+                        nc++;
+                        if (nc == 4 || c == 2 * k - 1) {
+                            if (T.posj) johnson_direct_masked<NW>(T, S, k, nc, cjob, cside);
+                            else johnson_direct<NW>(T, S, um, nc, cjob, cside);
+                            nc = 0;
+                        }
+                    }
+                }
+            }
             snode = nl;
             if (kids) {
 #pragma unroll
@@ -833,16 +867,16 @@ cudaError_t launch_requeue(const DevGroup* groups, int ngroups, cudaStream_t st)
 
 cudaError_t launch_bound(int nw, const DevInstance& I, int count, const int* sched, const int* l1, const int* l2,
                          int* wb, int* we, int* sb, int* se, int* nweak, int* nstrong, unsigned int* status,
-                         int ctas, int warps_per_cta, int smem, cudaStream_t st)
+                         int ctas, int warps_per_cta, int smem, cudaStream_t st, int method)
 {
     if (nw == 1) {
         cudaFuncSetAttribute(pbb_bound_kernel<1>, cudaFuncAttributeMaxDynamicSharedMemorySize, smem);
         pbb_bound_kernel<1><<<ctas, 32 * warps_per_cta, smem, st>>>(I, count, sched, l1, l2, wb, we, sb, se, nweak,
-                                                                     nstrong, status, warps_per_cta);
+                                                                     nstrong, status, warps_per_cta, method);
     } else {
         cudaFuncSetAttribute(pbb_bound_kernel<2>, cudaFuncAttributeMaxDynamicSharedMemorySize, smem);
         pbb_bound_kernel<2><<<ctas, 32 * warps_per_cta, smem, st>>>(I, count, sched, l1, l2, wb, we, sb, se, nweak,
-                                                                     nstrong, status, warps_per_cta);
+                                                                     nstrong, status, warps_per_cta, method);
     }
     return cudaGetLastError();
 }

@@ -14,5 +14,5 @@ cudaError_t launch_explore(int nw, const DevGroup* groups, int ngroups, int ctas
 cudaError_t launch_requeue(const DevGroup* groups, int ngroups, cudaStream_t st);
 cudaError_t launch_bound(int nw, const DevInstance& I, int count, const int* sched, const int* l1, const int* l2,
                          int* wb, int* we, int* sb, int* se, int* nweak, int* nstrong, unsigned int* status, int ctas,
-                         int warps_per_cta, int smem, cudaStream_t st);
+                         int warps_per_cta, int smem, cudaStream_t st, int method = 0);
 }  // namespace pbbl

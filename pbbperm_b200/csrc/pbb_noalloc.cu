@@ -258,6 +258,7 @@ extern "C" int pbb_bound_children_noalloc(const pbb_instance* inst, int32_t john
     I.n = n; I.m = m; I.P = P; I.Ppad = Ppad;
     I.p = pd; I.je = je; I.pm0 = pm; I.pm1 = pm + Ppad;
     I.min_arr = mt; I.min_dep = mt + m;
+    I.posj = nullptr;   // method 0 (sweeps over all positions) needs no position table
     const int warps = 8;
     const int smem = pbbl::smem_bytes(n, m, Ppad, warps);
     int sms = 0;

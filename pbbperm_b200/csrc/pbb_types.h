@@ -30,6 +30,7 @@ struct DevInstance {
     int Ppad;     // P rounded up to 32
     const int* p;                    // [m][n]
     const unsigned long long* je;    // [n][Ppad]
+    const unsigned char* posj;       // [n][Ppad] Johnson position of each job per pair (may be NULL)
     const unsigned char* pm0;        // [Ppad]
     const unsigned char* pm1;        // [Ppad]
     const int* min_arr;              // [m]
@@ -56,6 +57,8 @@ struct GroupCtl {
     // work of the Johnson sweeps: nodes swept, free jobs summed over them,
     // children evaluated by them (roofline accounting)
     unsigned long long jsweeps, jfree, jchild;
+    // children bounded by direct scans, and their free jobs summed
+    unsigned long long jdirect, jdirect_free;
 };
 
 // Explorer storage of a group (device memory, structure of arrays).
@@ -86,7 +89,7 @@ struct DevGroup {
 
 // Dynamic shared memory layout of one CTA (host and device agree).
 struct SmemPlan {
-    int je_off, p_off, pm0_off, pm1_off, marr_off, mdep_off, warp_off, warp_bytes, total;
+    int je_off, p_off, pm0_off, pm1_off, marr_off, mdep_off, posj_off, warp_off, warp_bytes, total;
 };
 
 __host__ __device__ inline int pbb_align(int x, int a) { return (x + a - 1) / a * a; }
@@ -103,6 +106,7 @@ __host__ __device__ inline SmemPlan pbb_smem_plan(int n, int m, int Ppad, int wa
     s.pm1_off = off;  off += pbb_align(Ppad, 16);
     s.marr_off = off; off += pbb_align(m * 4, 16);
     s.mdep_off = off; off += pbb_align(m * 4, 16);
+    s.posj_off = off; off += pbb_align(n * Ppad, 16);
     s.warp_off = off;
     s.warp_bytes = pbb_align((2 * PBB_MAX_N + 7 * 32) * 4 + 2 * PBB_MAX_N * m * 2 + 3 * PBB_MAX_N, 16);
     off += s.warp_bytes * warps;

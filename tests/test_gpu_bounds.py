@@ -9,14 +9,18 @@ from pbbperm_b200.instances import synthetic_instance
 pytestmark = pytest.mark.gpu
 
 
-def test_bound_children_vs_reference_golden(bounds_golden):
+@pytest.mark.parametrize("method", [None, 0, 1, 2])
+def test_bound_children_vs_reference_golden(bounds_golden, method):
+    """method None: the ABI entry point; 0: max-plus sweeps over all
+    positions; 1: direct per-child scans and 2: sweeps, both over the free
+    positions only, as the explorer runs them."""
     for case in bounds_golden["cases"]:
         p = np.array(case["p"], np.int32)
         nodes = case["nodes"]
         sched = np.array([nd["sched"] for nd in nodes], np.int32)
         l1 = np.array([nd["l1"] for nd in nodes], np.int32)
         l2 = np.array([nd["l2"] for nd in nodes], np.int32)
-        g = pb.bound_children(p, sched, l1, l2)
+        g = pb.bound_children(p, sched, l1, l2, method=method)
         for i, nd in enumerate(nodes):
             assert (g["weak_begin"][i] == nd["weak_begin"]).all(), (case["n"], case["m"], i)
             assert (g["weak_end"][i] == nd["weak_end"]).all(), (case["n"], case["m"], i)
@@ -36,13 +40,14 @@ def random_nodes(rng, n, count):
     return sched[keep], l1[keep], l2[keep]
 
 
+@pytest.mark.parametrize("method", [0, 1, 2])
 @pytest.mark.parametrize("n,m,seed", [(20, 20, 1), (50, 20, 2), (33, 5, 7), (64, 20, 8), (9, 2, 9), (17, 32, 10)])
-def test_bound_children_vs_oracle_random(n, m, seed):
+def test_bound_children_vs_oracle_random(n, m, seed, method):
     p = synthetic_instance(seed, n, m)
     O = Oracle(p)
     rng = np.random.default_rng(seed)
     sched, l1, l2 = random_nodes(rng, n, 300)
-    g = pb.bound_children(p, sched, l1, l2)
+    g = pb.bound_children(p, sched, l1, l2, method=method)
     for i in range(len(sched)):
         cb, ce, _, _ = O.weak_children(sched[i], l1[i], l2[i])
         assert (g["weak_begin"][i] == cb).all()
