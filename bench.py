@@ -44,6 +44,13 @@ def parse():
     ap.add_argument("--impl", default="ours", choices=["ours", "reference"])
     ap.add_argument("--e2e-steps", type=int, default=2)
     ap.add_argument("--cpu-sample", type=float, default=15.0)
+    ap.add_argument("--workload", default="nodes", choices=["nodes", "batch", "serve"],
+                    help="nodes: 50x20 nodes/s (default); batch: 512 uneven instances in one pool vs one at a "
+                         "time; serve: Poisson request stream through the pool vs each request alone")
+    ap.add_argument("--batch-count", type=int, default=512)
+    ap.add_argument("--rates", default="10,100,500,2000")
+    ap.add_argument("--serve-seconds", type=float, default=20.0)
+    ap.add_argument("--solo-sample", type=int, default=64)
     return ap.parse_args()
 
 

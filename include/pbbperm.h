@@ -110,6 +110,58 @@ int pbb_start_interval(pbb_engine* e, int32_t ub, const int32_t* root_perm, cons
 int pbb_set_ub(pbb_engine* e, int32_t ub);
 int pbb_get_result(pbb_engine* e, pbb_result* out);
 
+/* ------------------------------------------------------------------------
+ * Pool: many instances resident on one GPU at once (batched solving and
+ * continuous-batching serving).  No single counterpart in the reference; it
+ * runs the same explorer as pbb_solve (gpubb::next, gpu/src/gpubb.cu:273-395)
+ * for every resident instance inside one launch per window.
+ *
+ * Instances wait in a FIFO until a slot and enough explorer memory are free
+ * (footprint per instance = explorers x (row stride^2 + 5 x row stride + 20)
+ * bytes, row stride 32 for n <= 32 jobs, else 64).  Each pbb_pool_step
+ * admits what fits, runs one exploration window of `window_s` device seconds
+ * over all resident instances (one captured CUDA graph: explorer kernel,
+ * queue re-arm, status read-back), and retires the finished ones, whose
+ * results pbb_pool_poll returns.
+ * ------------------------------------------------------------------------ */
+typedef struct pbb_pool_config {
+    int32_t device;
+    int32_t max_jobs;            /* largest n accepted (<= 64); all instances share the row stride */
+    int32_t max_machines;        /* largest m accepted (<= 32) */
+    int32_t max_resident;        /* resident instances at most (0 = as many as CTAs fit) */
+    int32_t warps_per_cta;       /* block shape: warps per CTA (0 = 8) */
+    int32_t ctas_per_instance;   /* CTAs serving one instance in a window (0 = 1) */
+    int32_t explorers_per_warp;  /* explorers of an instance = ctas x warps x this (0 = 1) */
+    int32_t pad;
+    double window_s;             /* device time of one window (0 = 0.005) */
+    int64_t explorer_bytes;      /* explorer memory budget (0 = 1 GiB) */
+} pbb_pool_config;
+
+typedef struct pbb_pool_result {
+    int64_t tag;                 /* caller's tag of the submitted instance */
+    int32_t windows;             /* windows the instance was resident */
+    int32_t status;              /* PBB_OK, or an error code for this instance */
+    pbb_result result;
+} pbb_pool_result;
+
+typedef struct pbb_pool pbb_pool;
+
+void pbb_pool_config_default(pbb_pool_config* cfg);
+int pbb_pool_create(const pbb_pool_config* cfg, pbb_pool** out);
+int pbb_pool_destroy(pbb_pool* pool);
+/* Queue an instance (copied) with its search settings (bounding/branching
+ * mode, findAll, JohnsonMode of `search`; NULL = defaults), initial bound and
+ * root permutation (NULL = identity). */
+int pbb_pool_submit(pbb_pool* pool, const pbb_instance* inst, const pbb_config* search, int32_t ub,
+                    const int32_t* root_perm, int64_t tag);
+/* One window: admit, explore, retire.  Returns the counts left. */
+int pbb_pool_step(pbb_pool* pool, int32_t* resident, int32_t* queued);
+/* Move up to `max` finished results to `out`; *count = how many. */
+int pbb_pool_poll(pbb_pool* pool, pbb_pool_result* out, int32_t max, int32_t* count);
+/* Solve `count` instances to completion through one pool; results[i] for inst[i]. */
+int pbb_batch_solve(const pbb_instance* inst, int32_t count, const pbb_config* search, const int32_t* ubs,
+                    const pbb_pool_config* pool_cfg, pbb_result* results);
+
 /* Children bounds of `count` nodes of one instance.  Node i is the schedule
  * sched[i*n .. i*n+n) with jobs [0..limit1[i]] fixed in front and
  * [limit2[i]..n) fixed at the back.  Per job id (0 for fixed jobs):

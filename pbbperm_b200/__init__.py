@@ -73,6 +73,18 @@ class _Work(ctypes.Structure):
                 ("direct_children", ctypes.c_uint64), ("direct_free_jobs", ctypes.c_uint64)]
 
 
+class _PoolConfig(ctypes.Structure):
+    _fields_ = [("device", ctypes.c_int32), ("max_jobs", ctypes.c_int32), ("max_machines", ctypes.c_int32),
+                ("max_resident", ctypes.c_int32), ("warps_per_cta", ctypes.c_int32),
+                ("ctas_per_instance", ctypes.c_int32), ("explorers_per_warp", ctypes.c_int32),
+                ("pad", ctypes.c_int32), ("window_s", ctypes.c_double), ("explorer_bytes", ctypes.c_int64)]
+
+
+class _PoolResult(ctypes.Structure):
+    _fields_ = [("tag", ctypes.c_int64), ("windows", ctypes.c_int32), ("status", ctypes.c_int32),
+                ("result", _Result)]
+
+
 _lib = None
 
 
@@ -101,6 +113,16 @@ def lib():
         L.pbb_diag_bound_children.argtypes = [ctypes.POINTER(_Instance), ctypes.c_int32, ctypes.c_int32,
                                                ctypes.c_int32, ctypes.c_int32, _i32p, _i32p, _i32p, _i32p, _i32p,
                                                _i32p, _i32p, _i32p, _i32p]
+        L.pbb_pool_config_default.argtypes = [ctypes.POINTER(_PoolConfig)]
+        L.pbb_pool_create.argtypes = [ctypes.POINTER(_PoolConfig), ctypes.POINTER(ctypes.c_void_p)]
+        L.pbb_pool_destroy.argtypes = [ctypes.c_void_p]
+        L.pbb_pool_submit.argtypes = [ctypes.c_void_p, ctypes.POINTER(_Instance), ctypes.POINTER(_Config),
+                                      ctypes.c_int32, _i32p, ctypes.c_int64]
+        L.pbb_pool_step.argtypes = [ctypes.c_void_p, ctypes.POINTER(ctypes.c_int32), ctypes.POINTER(ctypes.c_int32)]
+        L.pbb_pool_poll.argtypes = [ctypes.c_void_p, ctypes.POINTER(_PoolResult), ctypes.c_int32,
+                                    ctypes.POINTER(ctypes.c_int32)]
+        L.pbb_batch_solve.argtypes = [ctypes.POINTER(_Instance), ctypes.c_int32, ctypes.POINTER(_Config), _i32p,
+                                      ctypes.POINTER(_PoolConfig), ctypes.POINTER(_Result)]
         L.pbb_diag_int32_peak.argtypes = [ctypes.c_int32, ctypes.POINTER(ctypes.c_double),
                                           ctypes.POINTER(ctypes.c_double)]
         _lib = L
@@ -276,3 +298,88 @@ def neh(p):
     cost = np.zeros(1, np.int32)
     _check(lib().pbb_neh(ctypes.byref(inst), _ptr(perm), _ptr(cost)))
     return int(cost[0]), perm
+
+
+class PoolConfig:
+    """Resident pool shape (include/pbbperm.h pbb_pool_config)."""
+
+    def __init__(self, max_jobs=32, max_machines=20, max_resident=0, warps_per_cta=8, ctas_per_instance=1,
+                 explorers_per_warp=1, window_s=0.005, explorer_bytes=1 << 30, device=0):
+        self.max_jobs = max_jobs
+        self.max_machines = max_machines
+        self.max_resident = max_resident
+        self.warps_per_cta = warps_per_cta
+        self.ctas_per_instance = ctas_per_instance
+        self.explorers_per_warp = explorers_per_warp
+        self.window_s = window_s
+        self.explorer_bytes = explorer_bytes
+        self.device = device
+
+    def _c(self):
+        return _PoolConfig(self.device, self.max_jobs, self.max_machines, self.max_resident, self.warps_per_cta,
+                           self.ctas_per_instance, self.explorers_per_warp, 0, self.window_s, self.explorer_bytes)
+
+
+class Pool:
+    """Many instances resident on one GPU; continuous batching by windows."""
+
+    def __init__(self, config=None):
+        self.config = config or PoolConfig()
+        h = ctypes.c_void_p()
+        c = self.config._c()
+        _check(lib().pbb_pool_create(ctypes.byref(c), ctypes.byref(h)))
+        self._h = h
+        self._inst = {}
+
+    def close(self):
+        if getattr(self, "_h", None):
+            lib().pbb_pool_destroy(self._h)
+            self._h = None
+
+    def __del__(self):
+        self.close()
+
+    def __enter__(self):
+        return self
+
+    def __exit__(self, *a):
+        self.close()
+
+    def submit(self, p, tag, ub=INF, config=None, root=None):
+        inst, pp = _instance(p)
+        cfg = (config or Config())._c()
+        root = None if root is None else np.ascontiguousarray(root, dtype=np.int32)
+        _check(lib().pbb_pool_submit(self._h, ctypes.byref(inst), ctypes.byref(cfg), int(ub), _ptr(root), int(tag)))
+
+    def step(self):
+        """One window; returns (resident, queued)."""
+        r = ctypes.c_int32(0)
+        q = ctypes.c_int32(0)
+        _check(lib().pbb_pool_step(self._h, ctypes.byref(r), ctypes.byref(q)))
+        return r.value, q.value
+
+    def poll(self, max_results=4096):
+        buf = (_PoolResult * max_results)()
+        got = ctypes.c_int32(0)
+        _check(lib().pbb_pool_poll(self._h, buf, max_results, ctypes.byref(got)))
+        out = []
+        for i in range(got.value):
+            d = _result(buf[i].result)
+            d["tag"] = buf[i].tag
+            d["windows"] = buf[i].windows
+            d["status"] = buf[i].status
+            out.append(d)
+        return out
+
+
+def batch_solve(instances, ubs=None, config=None, pool_config=None):
+    """Solve many instances through one resident pool (pbb_batch_solve)."""
+    cnt = len(instances)
+    keep = [np.ascontiguousarray(p, dtype=np.int32) for p in instances]
+    arr = (_Instance * cnt)(*[_Instance(p.shape[1], p.shape[0], _ptr(p)) for p in keep])
+    cfg = (config or Config())._c()
+    u = None if ubs is None else np.ascontiguousarray(ubs, dtype=np.int32)
+    res = (_Result * cnt)()
+    pc = None if pool_config is None else ctypes.byref(pool_config._c())
+    _check(lib().pbb_batch_solve(arr, cnt, ctypes.byref(cfg), _ptr(u), pc, res))
+    return [_result(r) for r in res]

@@ -574,12 +574,17 @@ __global__ void pbb_root_kernel(const DevGroup* groups, int ngroups, const int* 
 // or `budget_ns` of device time has passed, or `max_rounds` rounds.
 template <int NW>
 __global__ void __launch_bounds__(32 * PBB_WARPS_MAX, 1)
-pbb_explore_kernel(const DevGroup* groups, int ngroups, int warps_per_cta, unsigned long long budget_ns,
+pbb_explore_kernel(const DevGroup* groups, const int* ngroups_d, int warps_per_cta, unsigned long long budget_ns,
                    int max_rounds, int select_budget)
 {
     extern __shared__ __align__(16) unsigned char smem[];
+    // the group count lives in device memory so that a captured launch
+    // (fixed grid) serves any set of groups; CTAs past the last group exit
+    const int ngroups = *ngroups_d;
+    if (ngroups <= 0) return;
     const int gi = group_of_cta(groups, ngroups);
     const DevGroup G = groups[gi];
+    if ((int)blockIdx.x >= G.first_cta + G.ctas) return;
     const SmemPlan sp = pbb_smem_plan(G.inst.n, G.inst.m, G.inst.Ppad, warps_per_cta);
     CtaTables T;
     load_tables(G.inst, smem, sp, T);
@@ -660,8 +665,9 @@ __global__ void pbb_lower_ub_kernel(const DevGroup* groups, int g, int ub)
 
 // Between two launches: explorers waiting in the queue become idle again and
 // the queue is emptied (the next launch re-registers them).
-__global__ void pbb_requeue_kernel(const DevGroup* groups, int ngroups)
+__global__ void pbb_requeue_kernel(const DevGroup* groups, const int* ngroups_d)
 {
+    const int ngroups = *ngroups_d;
     for (int g = blockIdx.y; g < ngroups; g += gridDim.y) {
         const DevGroup G = groups[g];
         for (int id = blockIdx.x * blockDim.x + threadIdx.x; id < G.ivm.count; id += gridDim.x * blockDim.x) {
@@ -817,6 +823,19 @@ namespace pbbl {
 
 int smem_bytes(int n, int m, int Ppad, int warps) { return pbb_smem_plan(n, m, Ppad, warps).total; }
 
+int explore_ctas_per_sm(int nw, int warps_per_cta, int smem)
+{
+    int blocks = 0;
+    if (nw == 1) {
+        cudaFuncSetAttribute(pbb_explore_kernel<1>, cudaFuncAttributeMaxDynamicSharedMemorySize, smem);
+        cudaOccupancyMaxActiveBlocksPerMultiprocessor(&blocks, pbb_explore_kernel<1>, 32 * warps_per_cta, smem);
+    } else {
+        cudaFuncSetAttribute(pbb_explore_kernel<2>, cudaFuncAttributeMaxDynamicSharedMemorySize, smem);
+        cudaOccupancyMaxActiveBlocksPerMultiprocessor(&blocks, pbb_explore_kernel<2>, 32 * warps_per_cta, smem);
+    }
+    return blocks;
+}
+
 cudaError_t launch_reset(const DevGroup* groups, int ngroups, const int* ub, cudaStream_t st)
 {
     dim3 grid(64, ngroups < 65535 ? ngroups : 65535);
@@ -843,25 +862,25 @@ cudaError_t launch_lower_ub(const DevGroup* groups, int g, int ub, cudaStream_t 
     return cudaGetLastError();
 }
 
-cudaError_t launch_explore(int nw, const DevGroup* groups, int ngroups, int ctas, int warps_per_cta, int smem,
+cudaError_t launch_explore(int nw, const DevGroup* groups, const int* ngroups_d, int ctas, int warps_per_cta, int smem,
                            unsigned long long budget_ns, int max_rounds, int select_budget, cudaStream_t st)
 {
     if (nw == 1) {
         cudaFuncSetAttribute(pbb_explore_kernel<1>, cudaFuncAttributeMaxDynamicSharedMemorySize, smem);
-        pbb_explore_kernel<1><<<ctas, 32 * warps_per_cta, smem, st>>>(groups, ngroups, warps_per_cta, budget_ns,
+        pbb_explore_kernel<1><<<ctas, 32 * warps_per_cta, smem, st>>>(groups, ngroups_d, warps_per_cta, budget_ns,
                                                                        max_rounds, select_budget);
     } else {
         cudaFuncSetAttribute(pbb_explore_kernel<2>, cudaFuncAttributeMaxDynamicSharedMemorySize, smem);
-        pbb_explore_kernel<2><<<ctas, 32 * warps_per_cta, smem, st>>>(groups, ngroups, warps_per_cta, budget_ns,
+        pbb_explore_kernel<2><<<ctas, 32 * warps_per_cta, smem, st>>>(groups, ngroups_d, warps_per_cta, budget_ns,
                                                                        max_rounds, select_budget);
     }
     return cudaGetLastError();
 }
 
-cudaError_t launch_requeue(const DevGroup* groups, int ngroups, cudaStream_t st)
+cudaError_t launch_requeue(const DevGroup* groups, const int* ngroups_d, int max_groups, cudaStream_t st)
 {
-    dim3 grid(64, ngroups < 65535 ? ngroups : 65535);
-    pbb_requeue_kernel<<<grid, 256, 0, st>>>(groups, ngroups);
+    dim3 grid(64, max_groups < 65535 ? max_groups : 65535);
+    pbb_requeue_kernel<<<grid, 256, 0, st>>>(groups, ngroups_d);
     return cudaGetLastError();
 }
 

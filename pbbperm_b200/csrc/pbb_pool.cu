@@ -1,0 +1,525 @@
+// pbb_pool: many flow-shop instances resident on one GPU.  Each resident
+// instance is a group (tables, explorers, queue, counters) of the same
+// persistent explorer kernel the single-instance engine uses; one window
+// launch explores all of them.  Between windows the host retires finished
+// instances and admits queued ones by explorer-memory footprint, so requests
+// that arrive while others run join the next window (continuous batching).
+#include <cuda_runtime.h>
+#include <stdint.h>
+#include <string.h>
+
+#include <algorithm>
+#include <climits>
+#include <deque>
+#include <map>
+#include <vector>
+
+#include "pbb_types.h"
+#include "pbb_launch.h"
+#include "pbb_tables.h"
+#include "../../include/pbbperm.h"
+
+namespace {
+
+int pfail(int code, const char* msg)
+{
+    pbbh::set_error(msg);
+    return code;
+}
+
+#define PCK(call, what)                               \
+    do {                                              \
+        cudaError_t e_ = (call);                      \
+        if (e_ != cudaSuccess) {                      \
+            pbbh::set_error(what);                    \
+            return e_ == cudaErrorMemoryAllocation ? PBB_E_NOMEM : PBB_E_CUDA; \
+        }                                             \
+    } while (0)
+
+size_t align256(size_t x) { return (x + 255) / 256 * 256; }
+
+struct Request {
+    int64_t tag;
+    std::vector<int32_t> root;
+    pbb_config search;
+    int32_t ub;
+    pbbt::HostTables H;
+};
+
+struct Slot {
+    bool used = false;
+    int64_t tag = 0;
+    int n = 0, m = 0;
+    size_t off = 0, bytes = 0;      // explorer arena block
+    int explorers = 0;
+    int windows = 0;
+    DevGroup g{};
+};
+
+// first-fit allocator over the explorer arena
+struct Arena {
+    std::map<size_t, size_t> free_blocks;   // offset -> size
+    void init(size_t total) { free_blocks.clear(); free_blocks[0] = total; }
+    bool alloc(size_t bytes, size_t& off)
+    {
+        for (auto it = free_blocks.begin(); it != free_blocks.end(); ++it) {
+            if (it->second >= bytes) {
+                off = it->first;
+                const size_t rest = it->second - bytes;
+                free_blocks.erase(it);
+                if (rest) free_blocks[off + bytes] = rest;
+                return true;
+            }
+        }
+        return false;
+    }
+    void release(size_t off, size_t bytes)
+    {
+        auto it = free_blocks.emplace(off, bytes).first;
+        auto next = std::next(it);
+        if (next != free_blocks.end() && it->first + it->second == next->first) {
+            it->second += next->second;
+            free_blocks.erase(next);
+        }
+        if (it != free_blocks.begin()) {
+            auto prev = std::prev(it);
+            if (prev->first + prev->second == it->first) {
+                prev->second += it->second;
+                free_blocks.erase(it);
+            }
+        }
+    }
+};
+
+}  // namespace
+
+struct pbb_pool {
+    pbb_pool_config cfg{};
+    int dev = 0;
+    cudaStream_t st = nullptr;
+    int nw = 1, npad = 32, warps = 8, cpi = 1, epw = 1, smem = 0, root_smem = 0;
+    int max_slots = 0;          // resident instances at most
+    int grid = 0;               // CTAs of every window launch (max_slots x cpi)
+    int Ppad_max = 0;
+    size_t table_stride = 0;
+    size_t off_je = 0, off_p = 0, off_pm = 0, off_mt = 0, off_posj = 0;
+    unsigned char* arena = nullptr;
+    size_t arena_bytes = 0;
+    unsigned char* tables = nullptr;
+    GroupCtl* ctl = nullptr;
+    GroupCtl* ctl_h = nullptr;  // pinned mirror, written by the window graph
+    DevGroup* groups_d = nullptr;
+    int* ngroups_d = nullptr;
+    DevGroup* new_d = nullptr;
+    int* ub_d = nullptr;
+    int* roots_d = nullptr;
+    int* ivals_d = nullptr;
+    cudaGraphExec_t window = nullptr;
+    std::vector<Slot> slots;
+    std::deque<Request> queue;
+    std::vector<pbb_pool_result> done;
+    Arena alloc;
+    std::vector<int> pending_ub, pending_root;   // of the instances admitted in this step
+};
+
+extern "C" void pbb_pool_config_default(pbb_pool_config* c)
+{
+    if (!c) return;
+    memset(c, 0, sizeof(*c));
+    c->max_jobs = 32;
+    c->max_machines = 20;
+    c->warps_per_cta = 8;
+    c->ctas_per_instance = 1;
+    c->explorers_per_warp = 1;
+    c->window_s = 0.005;
+    c->explorer_bytes = (int64_t)1 << 30;
+}
+
+extern "C" int pbb_pool_destroy(pbb_pool* P)
+{
+    if (!P) return PBB_OK;
+    cudaSetDevice(P->dev);
+    if (P->st) cudaStreamSynchronize(P->st);
+    if (P->window) cudaGraphExecDestroy(P->window);
+    cudaFree(P->arena);
+    cudaFree(P->tables);
+    cudaFree(P->ctl);
+    cudaFreeHost(P->ctl_h);
+    cudaFree(P->groups_d);
+    cudaFree(P->ngroups_d);
+    cudaFree(P->new_d);
+    cudaFree(P->ub_d);
+    cudaFree(P->roots_d);
+    cudaFree(P->ivals_d);
+    if (P->st) cudaStreamDestroy(P->st);
+    delete P;
+    return PBB_OK;
+}
+
+namespace {
+
+size_t explorer_block_bytes(int E, int npad)
+{
+    size_t b = align256((size_t)E * npad * npad);     // mat
+    b += 5 * align256((size_t)E * npad);              // pos end dir pj bestperm
+    b += 5 * align256((size_t)E * 4);                 // line state bestcost qseq qval
+    return b;
+}
+
+void carve_explorers(unsigned char* base, int E, int npad, DevIvms& V)
+{
+    size_t o = 0;
+    V.count = E;
+    V.npad = npad;
+    V.mat = reinterpret_cast<signed char*>(base + o); o += align256((size_t)E * npad * npad);
+    V.pos = reinterpret_cast<signed char*>(base + o); o += align256((size_t)E * npad);
+    V.end = reinterpret_cast<signed char*>(base + o); o += align256((size_t)E * npad);
+    V.dir = reinterpret_cast<signed char*>(base + o); o += align256((size_t)E * npad);
+    V.pj = reinterpret_cast<signed char*>(base + o); o += align256((size_t)E * npad);
+    V.bestperm = reinterpret_cast<signed char*>(base + o); o += align256((size_t)E * npad);
+    V.line = reinterpret_cast<int*>(base + o); o += align256((size_t)E * 4);
+    V.state = reinterpret_cast<int*>(base + o); o += align256((size_t)E * 4);
+    V.bestcost = reinterpret_cast<int*>(base + o); o += align256((size_t)E * 4);
+    V.qseq = reinterpret_cast<unsigned*>(base + o); o += align256((size_t)E * 4);
+    V.qval = reinterpret_cast<int*>(base + o);
+}
+
+int pool_create(const pbb_pool_config* in, pbb_pool* P)
+{
+    pbb_pool_config c;
+    pbb_pool_config_default(&c);
+    if (in) {
+        c = *in;
+        pbb_pool_config d;
+        pbb_pool_config_default(&d);
+        if (c.warps_per_cta <= 0) c.warps_per_cta = d.warps_per_cta;
+        if (c.ctas_per_instance <= 0) c.ctas_per_instance = d.ctas_per_instance;
+        if (c.explorers_per_warp <= 0) c.explorers_per_warp = d.explorers_per_warp;
+        if (c.window_s <= 0) c.window_s = d.window_s;
+        if (c.explorer_bytes <= 0) c.explorer_bytes = d.explorer_bytes;
+    }
+    if (c.max_jobs < 2 || c.max_jobs > PBB_MAX_JOBS) return pfail(PBB_E_INVAL, "max_jobs must be in [2, 64]");
+    if (c.max_machines < 2 || c.max_machines > PBB_MAX_MACHINES)
+        return pfail(PBB_E_INVAL, "max_machines must be in [2, 32]");
+    if (c.warps_per_cta > PBB_WARPS_MAX) return pfail(PBB_E_INVAL, "warps_per_cta must be <= 24");
+    if (c.window_s > 120.0) return pfail(PBB_E_INVAL, "window_s must be <= 120");
+    P->cfg = c;
+    P->dev = c.device;
+    PCK(cudaSetDevice(P->dev), "cudaSetDevice failed");
+    PCK(cudaStreamCreateWithFlags(&P->st, cudaStreamNonBlocking), "stream creation failed");
+    P->nw = c.max_jobs <= 32 ? 1 : 2;
+    P->npad = 32 * P->nw;
+    P->warps = c.warps_per_cta;
+    P->cpi = c.ctas_per_instance;
+    P->epw = c.explorers_per_warp;
+    const int Pmax = c.max_machines * (c.max_machines - 1) / 2;
+    P->Ppad_max = (Pmax + 31) / 32 * 32;
+    P->smem = pbbl::smem_bytes(c.max_jobs, c.max_machines, P->Ppad_max, P->warps);
+    P->root_smem = pbbl::smem_bytes(c.max_jobs, c.max_machines, P->Ppad_max, 1);
+    int optin = 0, sms = 0;
+    cudaDeviceGetAttribute(&optin, cudaDevAttrMaxSharedMemoryPerBlockOptin, P->dev);
+    cudaDeviceGetAttribute(&sms, cudaDevAttrMultiProcessorCount, P->dev);
+    if (P->smem > optin) return pfail(PBB_E_INVAL, "tables of max_jobs x max_machines do not fit in shared memory");
+    const int per_sm = pbbl::explore_ctas_per_sm(P->nw, P->warps, P->smem);
+    if (per_sm < 1) return pfail(PBB_E_INVAL, "explorer kernel cannot be resident with this block shape");
+    int capacity = sms * per_sm / P->cpi;
+    if (capacity < 1) capacity = 1;
+    P->max_slots = c.max_resident > 0 ? std::min(c.max_resident, capacity) : capacity;
+    P->grid = P->max_slots * P->cpi;
+    // per-slot instance tables
+    P->off_je = 0;
+    P->off_p = align256(P->off_je + (size_t)c.max_jobs * P->Ppad_max * 8);
+    P->off_pm = align256(P->off_p + (size_t)c.max_jobs * c.max_machines * 4);
+    P->off_mt = align256(P->off_pm + 2 * (size_t)P->Ppad_max);
+    P->off_posj = align256(P->off_mt + 2 * (size_t)c.max_machines * 4);
+    P->table_stride = align256(P->off_posj + (size_t)c.max_jobs * P->Ppad_max);
+    const int S = P->max_slots;
+    PCK(cudaMalloc(&P->tables, P->table_stride * S), "table memory");
+    PCK(cudaMalloc(&P->ctl, sizeof(GroupCtl) * S), "control blocks");
+    PCK(cudaMemset(P->ctl, 0, sizeof(GroupCtl) * S), "control blocks");
+    PCK(cudaMallocHost(&P->ctl_h, sizeof(GroupCtl) * S), "pinned control mirror");
+    memset(P->ctl_h, 0, sizeof(GroupCtl) * S);
+    PCK(cudaMalloc(&P->groups_d, sizeof(DevGroup) * S), "group list");
+    PCK(cudaMalloc(&P->new_d, sizeof(DevGroup) * S), "group list");
+    PCK(cudaMalloc(&P->ngroups_d, sizeof(int)), "group count");
+    PCK(cudaMemset(P->ngroups_d, 0, sizeof(int)), "group count");
+    PCK(cudaMalloc(&P->ub_d, sizeof(int) * S), "bounds");
+    PCK(cudaMalloc(&P->roots_d, sizeof(int) * S * PBB_MAX_N), "roots");
+    PCK(cudaMalloc(&P->ivals_d, sizeof(int) * S * 2 * PBB_MAX_N), "intervals");
+    P->arena_bytes = (size_t)c.explorer_bytes;
+    const int E = P->cpi * P->warps * P->epw;
+    if (explorer_block_bytes(E, P->npad) > P->arena_bytes)
+        return pfail(PBB_E_INVAL, "explorer_bytes is smaller than one instance's footprint");
+    PCK(cudaMalloc(&P->arena, P->arena_bytes), "explorer memory");
+    P->alloc.init(P->arena_bytes);
+    P->slots.assign(S, Slot());
+    // the window: explorer kernel, queue re-arm, control read-back, as one graph
+    cudaGraph_t graph = nullptr;
+    const unsigned long long budget = (unsigned long long)(c.window_s * 1e9);
+    PCK(cudaStreamBeginCapture(P->st, cudaStreamCaptureModeRelaxed), "graph capture");
+    cudaError_t e1 = pbbl::launch_explore(P->nw, P->groups_d, P->ngroups_d, P->grid, P->warps, P->smem, budget,
+                                          INT_MAX, 4096, P->st);
+    cudaError_t e2 = pbbl::launch_requeue(P->groups_d, P->ngroups_d, S, P->st);
+    cudaError_t e3 = cudaMemcpyAsync(P->ctl_h, P->ctl, sizeof(GroupCtl) * S, cudaMemcpyDeviceToHost, P->st);
+    cudaError_t e4 = cudaStreamEndCapture(P->st, &graph);
+    if (e1 || e2 || e3 || e4) {
+        if (graph) cudaGraphDestroy(graph);
+        return pfail(PBB_E_CUDA, "capturing the window graph failed");
+    }
+    cudaError_t e5 = cudaGraphInstantiate(&P->window, graph, 0);
+    cudaGraphDestroy(graph);
+    if (e5) return pfail(PBB_E_CUDA, "instantiating the window graph failed");
+    return PBB_OK;
+}
+
+}  // namespace
+
+extern "C" int pbb_pool_create(const pbb_pool_config* cfg, pbb_pool** out)
+{
+    if (!out) return pfail(PBB_E_INVAL, "out is NULL");
+    *out = nullptr;
+    pbb_pool* P = new pbb_pool();
+    const int rc = pool_create(cfg, P);
+    if (rc) {
+        pbb_pool_destroy(P);
+        return rc;
+    }
+    *out = P;
+    return PBB_OK;
+}
+
+extern "C" int pbb_pool_submit(pbb_pool* P, const pbb_instance* inst, const pbb_config* search, int32_t ub,
+                               const int32_t* root_perm, int64_t tag)
+{
+    if (!P) return pfail(PBB_E_INVAL, "pool is NULL");
+    if (!inst || !inst->p) return pfail(PBB_E_INVAL, "instance is NULL");
+    if (inst->n_jobs > P->cfg.max_jobs || inst->n_machines > P->cfg.max_machines)
+        return pfail(PBB_E_INVAL, "instance larger than the pool's max_jobs x max_machines");
+    if (ub < 0) return pfail(PBB_E_INVAL, "ub must be >= 0");
+    Request r;
+    r.tag = tag;
+    pbb_config_default(&r.search);
+    if (search) r.search = *search;
+    const pbb_config& c = r.search;
+    if (c.bounding_mode < 0 || c.bounding_mode > 2) return pfail(PBB_E_INVAL, "boundingMode must be 0, 1 or 2");
+    if (!(c.branching_mode == -3 || c.branching_mode == -2 || c.branching_mode == -1 || c.branching_mode == 1 ||
+          c.branching_mode == 2 || c.branching_mode == 3))
+        return pfail(PBB_E_INVAL, "adaptiveBranchingMode must be one of -3,-2,-1,1,2,3");
+    if (c.early_stop_johnson) return pfail(PBB_E_UNSUPPORTED, "earlyStopJohnson=true is not supported");
+    if (c.sorted_dfs) return pfail(PBB_E_UNSUPPORTED, "sortedDFS != 0 is not supported");
+    const int rc = pbbt::build_tables(inst, c.johnson_mode, r.H);
+    if (rc) return rc;
+    const int n = inst->n_jobs;
+    r.root.assign(PBB_MAX_N, 0);
+    std::vector<int> seen(n, 0);
+    for (int i = 0; i < n; i++) {
+        const int j = root_perm ? root_perm[i] : i;
+        if (j < 0 || j >= n || seen[j]) return pfail(PBB_E_INVAL, "root_perm is not a permutation of 0..n-1");
+        seen[j] = 1;
+        r.root[i] = j;
+    }
+    r.ub = ub;
+    P->queue.push_back(std::move(r));
+    return PBB_OK;
+}
+
+namespace {
+
+// admit queued instances while a slot and explorer memory are free (FIFO)
+int admit(pbb_pool* P, std::vector<int>& admitted)
+{
+    const int E = P->cpi * P->warps * P->epw;
+    const size_t bytes = explorer_block_bytes(E, P->npad);
+    while (!P->queue.empty()) {
+        int s = -1;
+        for (int i = 0; i < P->max_slots; i++)
+            if (!P->slots[i].used) { s = i; break; }
+        if (s < 0) break;
+        size_t off = 0;
+        if (!P->alloc.alloc(bytes, off)) break;
+        Request& r = P->queue.front();
+        const pbbt::HostTables& H = r.H;
+        unsigned char* tb = P->tables + (size_t)s * P->table_stride;
+        PCK(cudaMemcpyAsync(tb + P->off_je, H.je.data(), H.je.size() * 8, cudaMemcpyHostToDevice, P->st), "upload");
+        PCK(cudaMemcpyAsync(tb + P->off_p, H.p.data(), H.p.size() * 4, cudaMemcpyHostToDevice, P->st), "upload");
+        PCK(cudaMemcpyAsync(tb + P->off_pm, H.pm0.data(), H.Ppad, cudaMemcpyHostToDevice, P->st), "upload");
+        PCK(cudaMemcpyAsync(tb + P->off_pm + H.Ppad, H.pm1.data(), H.Ppad, cudaMemcpyHostToDevice, P->st), "upload");
+        PCK(cudaMemcpyAsync(tb + P->off_mt, H.min_arr.data(), H.m * 4, cudaMemcpyHostToDevice, P->st), "upload");
+        PCK(cudaMemcpyAsync(tb + P->off_mt + H.m * 4, H.min_dep.data(), H.m * 4, cudaMemcpyHostToDevice, P->st),
+            "upload");
+        PCK(cudaMemcpyAsync(tb + P->off_posj, H.posj.data(), H.posj.size(), cudaMemcpyHostToDevice, P->st), "upload");
+        Slot& sl = P->slots[s];
+        sl = Slot();
+        sl.used = true;
+        sl.tag = r.tag;
+        sl.n = H.n;
+        sl.m = H.m;
+        sl.off = off;
+        sl.bytes = bytes;
+        sl.explorers = E;
+        DevGroup& g = sl.g;
+        g.inst.n = H.n; g.inst.m = H.m; g.inst.P = H.P; g.inst.Ppad = H.Ppad;
+        g.inst.p = reinterpret_cast<const int*>(tb + P->off_p);
+        g.inst.je = reinterpret_cast<const unsigned long long*>(tb + P->off_je);
+        g.inst.pm0 = tb + P->off_pm;
+        g.inst.pm1 = tb + P->off_pm + H.Ppad;
+        g.inst.min_arr = reinterpret_cast<const int*>(tb + P->off_mt);
+        g.inst.min_dep = reinterpret_cast<const int*>(tb + P->off_mt + H.m * 4);
+        g.inst.posj = tb + P->off_posj;
+        g.search.bound_mode = r.search.bounding_mode;
+        g.search.branch_mode = r.search.branching_mode;
+        g.search.find_all = r.search.find_all ? 1 : 0;
+        carve_explorers(P->arena + off, E, P->npad, g.ivm);
+        g.ctl = P->ctl + s;
+        admitted.push_back(s);
+        P->pending_ub.push_back(r.ub);
+        P->pending_root.insert(P->pending_root.end(), r.root.begin(), r.root.end());
+        P->queue.pop_front();
+    }
+    return PBB_OK;
+}
+
+}  // namespace
+
+extern "C" int pbb_pool_step(pbb_pool* P, int32_t* resident, int32_t* queued)
+{
+    if (!P) return pfail(PBB_E_INVAL, "pool is NULL");
+    PCK(cudaSetDevice(P->dev), "cudaSetDevice failed");
+    std::vector<int> admitted;
+    P->pending_ub.clear();
+    P->pending_root.clear();
+    int rc = admit(P, admitted);
+    if (rc) return rc;
+    const int na = (int)admitted.size();
+    if (na > 0) {
+        // empty explorers, reset counters, bound the roots of the newcomers
+        std::vector<DevGroup> ng(na);
+        std::vector<int> iv((size_t)na * 2 * PBB_MAX_N, 0);
+        for (int i = 0; i < na; i++) {
+            const Slot& sl = P->slots[admitted[i]];
+            ng[i] = sl.g;
+            for (int e = 0; e < sl.n; e++) {
+                iv[(size_t)(2 * i) * PBB_MAX_N + e] = 0;
+                iv[(size_t)(2 * i + 1) * PBB_MAX_N + e] = sl.n - 1 - e;
+            }
+        }
+        PCK(cudaMemcpyAsync(P->new_d, ng.data(), sizeof(DevGroup) * na, cudaMemcpyHostToDevice, P->st), "upload");
+        PCK(cudaMemcpyAsync(P->ub_d, P->pending_ub.data(), sizeof(int) * na, cudaMemcpyHostToDevice, P->st),
+            "upload");
+        PCK(cudaMemcpyAsync(P->roots_d, P->pending_root.data(), sizeof(int) * na * PBB_MAX_N,
+                            cudaMemcpyHostToDevice, P->st), "upload");
+        PCK(cudaMemcpyAsync(P->ivals_d, iv.data(), sizeof(int) * iv.size(), cudaMemcpyHostToDevice, P->st),
+            "upload");
+        PCK(pbbl::launch_reset(P->new_d, na, P->ub_d, P->st), "reset launch");
+        PCK(pbbl::launch_root(P->nw, P->new_d, na, P->roots_d, P->ivals_d, PBB_MAX_N, P->root_smem, P->st),
+            "root launch");
+    }
+    // the window over every resident instance
+    std::vector<DevGroup> act;
+    std::vector<int> act_slot;
+    for (int s = 0; s < P->max_slots; s++) {
+        if (!P->slots[s].used) continue;
+        DevGroup g = P->slots[s].g;
+        g.first_cta = (int)act.size() * P->cpi;
+        g.ctas = P->cpi;
+        act.push_back(g);
+        act_slot.push_back(s);
+    }
+    const int nact = (int)act.size();
+    if (nact > 0) {
+        PCK(cudaMemcpyAsync(P->groups_d, act.data(), sizeof(DevGroup) * nact, cudaMemcpyHostToDevice, P->st),
+            "upload");
+    }
+    PCK(cudaMemcpyAsync(P->ngroups_d, &nact, sizeof(int), cudaMemcpyHostToDevice, P->st), "upload");
+    if (nact > 0) PCK(cudaGraphLaunch(P->window, P->st), "window launch");
+    PCK(cudaStreamSynchronize(P->st), "window");
+    // retire the finished instances
+    for (int i = 0; i < nact; i++) {
+        const int s = act_slot[i];
+        Slot& sl = P->slots[s];
+        sl.windows++;
+        const GroupCtl& c = P->ctl_h[s];
+        if (c.active != 0) continue;
+        pbb_pool_result pr;
+        memset(&pr, 0, sizeof(pr));
+        pr.tag = sl.tag;
+        pr.windows = sl.windows;
+        pr.status = (c.status & PBB_ST_BADINPUT) ? PBB_E_INVAL : PBB_OK;
+        pbb_result& r = pr.result;
+        const unsigned id = (unsigned)(c.best_key & 0xffffffffull);
+        r.complete = 1;
+        r.found = (c.found > 0 && id != 0xffffffffu && id < (unsigned)sl.explorers) ? 1 : 0;
+        r.cost = (int32_t)(c.best_key >> 32);
+        r.n_jobs = sl.n;
+        r.stats.decomposed = c.decomposed;
+        r.stats.johnson_bounds = c.johnson_bounds;
+        r.stats.simple_bounds = c.simple_bounds;
+        r.stats.leaves = c.leaves;
+        r.stats.steals = c.steals;
+        if (r.found) {
+            signed char buf[PBB_MAX_N];
+            PCK(cudaMemcpy(buf, sl.g.ivm.bestperm + (size_t)id * sl.g.ivm.npad, sl.n, cudaMemcpyDeviceToHost),
+                "result read-back");
+            for (int j = 0; j < sl.n; j++) r.perm[j] = buf[j];
+        }
+        P->done.push_back(pr);
+        P->alloc.release(sl.off, sl.bytes);
+        sl = Slot();
+    }
+    int res = 0;
+    for (int s = 0; s < P->max_slots; s++) res += P->slots[s].used ? 1 : 0;
+    if (resident) *resident = res;
+    if (queued) *queued = (int32_t)P->queue.size();
+    return PBB_OK;
+}
+
+extern "C" int pbb_pool_poll(pbb_pool* P, pbb_pool_result* out, int32_t max, int32_t* count)
+{
+    if (!P || (!out && max > 0)) return pfail(PBB_E_INVAL, "NULL argument");
+    const int k = std::min((int)P->done.size(), (int)std::max(0, max));
+    for (int i = 0; i < k; i++) out[i] = P->done[i];
+    P->done.erase(P->done.begin(), P->done.begin() + k);
+    if (count) *count = k;
+    return PBB_OK;
+}
+
+extern "C" int pbb_batch_solve(const pbb_instance* inst, int32_t count, const pbb_config* search, const int32_t* ubs,
+                               const pbb_pool_config* pool_cfg, pbb_result* results)
+{
+    if (count < 0 || (count > 0 && (!inst || !results))) return pfail(PBB_E_INVAL, "bad arguments");
+    if (count == 0) return PBB_OK;
+    pbb_pool_config c;
+    if (pool_cfg) {
+        c = *pool_cfg;
+    } else {
+        pbb_pool_config_default(&c);
+        c.max_jobs = 2;
+        c.max_machines = 2;
+        for (int i = 0; i < count; i++) {
+            c.max_jobs = std::max(c.max_jobs, (int32_t)inst[i].n_jobs);
+            c.max_machines = std::max(c.max_machines, (int32_t)inst[i].n_machines);
+        }
+        c.window_s = 0.02;
+    }
+    pbb_pool* P = nullptr;
+    int rc = pbb_pool_create(&c, &P);
+    if (rc) return rc;
+    for (int i = 0; i < count && !rc; i++) rc = pbb_pool_submit(P, &inst[i], search, ubs ? ubs[i] : INT32_MAX, nullptr, i);
+    int32_t res = 0, q = count;
+    std::vector<pbb_pool_result> out(count);
+    int got_total = 0;
+    while (!rc && (res > 0 || q > 0 || got_total < count)) {
+        rc = pbb_pool_step(P, &res, &q);
+        if (rc) break;
+        int32_t got = 0;
+        rc = pbb_pool_poll(P, out.data(), count, &got);
+        for (int i = 0; i < got; i++) {
+            const int64_t t = out[i].tag;
+            if (t >= 0 && t < count) results[t] = out[i].result;
+        }
+        got_total += got;
+        if (res == 0 && q == 0) break;
+    }
+    pbb_pool_destroy(P);
+    return rc;
+}

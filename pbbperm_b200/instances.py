@@ -58,3 +58,52 @@ def write_vrf(path, p):
         f.write("%d %d\n" % (n, m))
         for j in range(n):
             f.write(" ".join("%d %d" % (k, p[k, j]) for k in range(m)) + "\n")
+
+
+def _draw(state, lo, hi):
+    span = hi - lo + 1
+    limit = _M64 - (_M64 % span)
+    while True:
+        state, u = _splitmix64(state)
+        if u < limit:
+            return state, lo + (u % span)
+
+
+def batch_instance(seed):
+    """Instance of the batched workload: n uniform in {12..20} jobs and m in
+    {5, 10, 20} machines drawn first from the seed's splitmix64 stream, then
+    U[1,99] processing times from the same stream (row-major m x n)."""
+    s = seed & _M64
+    s, n = _draw(s, 12, 20)
+    s, k = _draw(s, 0, 2)
+    m = (5, 10, 20)[k]
+    p = np.empty(n * m, dtype=np.int32)
+    for i in range(n * m):
+        s, p[i] = _draw(s, 1, 99)
+    return p.reshape(m, n)
+
+
+def serving_instance(seed):
+    """Instance of the serving workload: n uniform in {10..22}, m uniform in
+    {5..20}, then U[1,99] times, all from the seed's splitmix64 stream."""
+    s = seed & _M64
+    s, n = _draw(s, 10, 22)
+    s, m = _draw(s, 5, 20)
+    p = np.empty(n * m, dtype=np.int32)
+    for i in range(n * m):
+        s, p[i] = _draw(s, 1, 99)
+    return p.reshape(m, n)
+
+
+def poisson_arrivals(seed, rate, count):
+    """Arrival times (s) of a Poisson stream: exponential gaps of mean 1/rate
+    from the seed's splitmix64 stream (53-bit uniforms)."""
+    s = seed & _M64
+    t = 0.0
+    out = np.empty(count)
+    for i in range(count):
+        s, u = _splitmix64(s)
+        x = ((u >> 11) + 1) / float(1 << 53)   # (0, 1]
+        t += -np.log(x) / rate
+        out[i] = t
+    return out
