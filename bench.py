@@ -219,7 +219,7 @@ def run_ours(args):
             dn, ds, done, res = window()
             nodes += dn
             dev_s += ds
-            launches += 2          # explorer kernel + queue re-arm kernel
+            launches += 1          # the explorer kernel (idle queue persists across launches)
             steps_done += 1
             exchange_ub(res)
         torch.cuda.synchronize()

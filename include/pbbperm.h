@@ -117,8 +117,8 @@ int pbb_get_result(pbb_engine* e, pbb_result* out);
  * for every resident instance inside one launch per window.
  *
  * Instances wait in a FIFO until a slot and enough explorer memory are free
- * (footprint per instance = explorers x (row stride^2 + 5 x row stride + 20)
- * bytes, row stride 32 for n <= 32 jobs, else 64).  Each pbb_pool_step
+ * (footprint per instance = explorers x (row stride^2 + 5 x row stride + 20
+ * + 384 x row stride) bytes, row stride 32 for n <= 32 jobs, else 64).  Each pbb_pool_step
  * admits what fits, runs one exploration window of `window_s` device seconds
  * over all resident instances (one captured CUDA graph: explorer kernel,
  * queue re-arm, status read-back), and retires the finished ones, whose
@@ -130,11 +130,12 @@ typedef struct pbb_pool_config {
     int32_t max_machines;        /* largest m accepted (<= 32) */
     int32_t max_resident;        /* resident instances at most (0 = as many as CTAs fit) */
     int32_t warps_per_cta;       /* block shape: warps per CTA (0 = 8) */
-    int32_t ctas_per_instance;   /* CTAs serving one instance in a window (0 = 1) */
-    int32_t explorers_per_warp;  /* explorers of an instance = ctas x warps x this (0 = 1) */
+    int32_t ctas_per_instance;   /* cap on the CTAs one instance gets in a window (0 = none); every
+                                    window spreads all resident CTAs evenly over the instances */
+    int32_t explorers_per_instance; /* explorers (IVMs) of each instance (0 = 1024) */
     int32_t pad;
     double window_s;             /* device time of one window (0 = 0.005) */
-    int64_t explorer_bytes;      /* explorer memory budget (0 = 1 GiB) */
+    int64_t explorer_bytes;      /* explorer memory budget (0 = 8 GiB) */
 } pbb_pool_config;
 
 typedef struct pbb_pool_result {

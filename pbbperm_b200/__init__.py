@@ -76,7 +76,7 @@ class _Work(ctypes.Structure):
 class _PoolConfig(ctypes.Structure):
     _fields_ = [("device", ctypes.c_int32), ("max_jobs", ctypes.c_int32), ("max_machines", ctypes.c_int32),
                 ("max_resident", ctypes.c_int32), ("warps_per_cta", ctypes.c_int32),
-                ("ctas_per_instance", ctypes.c_int32), ("explorers_per_warp", ctypes.c_int32),
+                ("ctas_per_instance", ctypes.c_int32), ("explorers_per_instance", ctypes.c_int32),
                 ("pad", ctypes.c_int32), ("window_s", ctypes.c_double), ("explorer_bytes", ctypes.c_int64)]
 
 
@@ -303,21 +303,22 @@ def neh(p):
 class PoolConfig:
     """Resident pool shape (include/pbbperm.h pbb_pool_config)."""
 
-    def __init__(self, max_jobs=32, max_machines=20, max_resident=0, warps_per_cta=8, ctas_per_instance=1,
-                 explorers_per_warp=1, window_s=0.005, explorer_bytes=1 << 30, device=0):
+    def __init__(self, max_jobs=32, max_machines=20, max_resident=0, warps_per_cta=8, ctas_per_instance=0,
+                 explorers_per_instance=1024, window_s=0.005, explorer_bytes=8 << 30, device=0):
         self.max_jobs = max_jobs
         self.max_machines = max_machines
         self.max_resident = max_resident
         self.warps_per_cta = warps_per_cta
         self.ctas_per_instance = ctas_per_instance
-        self.explorers_per_warp = explorers_per_warp
+        self.explorers_per_instance = explorers_per_instance
         self.window_s = window_s
         self.explorer_bytes = explorer_bytes
         self.device = device
 
     def _c(self):
         return _PoolConfig(self.device, self.max_jobs, self.max_machines, self.max_resident, self.warps_per_cta,
-                           self.ctas_per_instance, self.explorers_per_warp, 0, self.window_s, self.explorer_bytes)
+                           self.ctas_per_instance, self.explorers_per_instance, 0, self.window_s,
+                           self.explorer_bytes)
 
 
 class Pool:

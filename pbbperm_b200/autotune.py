@@ -1,8 +1,8 @@
 """Autotuner of the resident pool's shape for a batch of instances.
 
 Times pbb_batch_solve on a calibration sample (every k-th instance of the
-batch, same bounds) for each candidate block shape (warps per CTA), explorers
-per warp and CTAs per instance, and returns the fastest PoolConfig with the
+batch, same bounds) for each candidate block shape (warps per CTA) and explorers
+per instance, and returns the fastest PoolConfig with the
 timings of all candidates.
 """
 import itertools
@@ -12,8 +12,7 @@ import pbbperm_b200 as pb
 
 CANDIDATES = {
     "warps_per_cta": (4, 8, 16),
-    "explorers_per_warp": (1, 2),
-    "ctas_per_instance": (1, 2),
+    "explorers_per_instance": (256, 1024, 4096),
 }
 
 
@@ -23,16 +22,15 @@ def tune_pool(instances, ubs, search, max_jobs, max_machines, sample=48, window_
     cal_ub = ubs[::step][:sample]
     trials = []
     best = None
-    for w, e, c in itertools.product(CANDIDATES["warps_per_cta"], CANDIDATES["explorers_per_warp"],
-                                     CANDIDATES["ctas_per_instance"]):
-        pc = pb.PoolConfig(max_jobs=max_jobs, max_machines=max_machines, warps_per_cta=w, explorers_per_warp=e,
-                           ctas_per_instance=c, window_s=window_s, device=device)
+    for w, e in itertools.product(CANDIDATES["warps_per_cta"], CANDIDATES["explorers_per_instance"]):
+        pc = pb.PoolConfig(max_jobs=max_jobs, max_machines=max_machines, warps_per_cta=w, explorers_per_instance=e,
+                           window_s=window_s, device=device)
         t = float("inf")
         for _ in range(repeats):
             t0 = time.perf_counter()
             pb.batch_solve(cal, ubs=cal_ub, config=search, pool_config=pc)
             t = min(t, time.perf_counter() - t0)
-        trials.append(dict(warps_per_cta=w, explorers_per_warp=e, ctas_per_instance=c, seconds=round(t, 4)))
+        trials.append(dict(warps_per_cta=w, explorers_per_instance=e, seconds=round(t, 4)))
         if best is None or t < best[0]:
             best = (t, pc)
     return best[1], trials

@@ -195,6 +195,78 @@ __device__ __forceinline__ void partial_schedule(const CtaTables& T, const WarpS
     __syncwarp();
 }
 
+// ---------------------------------------------------------------------------
+// path partial schedule kept one machine per lane (lane k = machine k):
+//   hf = heads of the front jobs, hb = tails of the back jobs (both zero
+//   based), hr = loads of the free jobs.  Going down one level adds one job
+//   to the front or to the back; both updates are exact max-plus scans.
+// ---------------------------------------------------------------------------
+
+// heads after appending job u: h_k = max(h_{k-1}, hf_k) + p_k(u), h_{-1} = 0,
+// equal to P_k + max_{j<=k}(hf_j - P_{j-1}) with P the prefix sums of p(u)
+// (heads are >= 0, so the h_{-1} term never wins)
+__device__ __forceinline__ int append_front(const CtaTables& T, int hf, int u)
+{
+    const int lane = lane_id();
+    const int pu = lane < T.m ? T.p[lane * T.n + u] : 0;
+    int P = pu;
+#pragma unroll
+    for (int o = 1; o < 32; o <<= 1) {
+        const int t = __shfl_up_sync(FULLMASK, P, o);
+        if (lane >= o) P += t;
+    }
+    int x = hf - (P - pu);
+#pragma unroll
+    for (int o = 1; o < 32; o <<= 1) {
+        const int t = __shfl_up_sync(FULLMASK, x, o);
+        if (lane >= o) x = max(x, t);
+    }
+    return P + x;
+}
+
+// tails after putting job u first among the back jobs:
+// t_k = max(t_{k+1}, hb_k) + p_k(u), t_m = 0, equal to
+// Q_k + max_{j>=k}(hb_j - Q_{j+1}) with Q the suffix sums of p(u)
+__device__ __forceinline__ int prepend_back(const CtaTables& T, int hb, int u)
+{
+    const int lane = lane_id();
+    const bool on = lane < T.m;
+    const int pu = on ? T.p[lane * T.n + u] : 0;
+    int Q = pu;
+#pragma unroll
+    for (int o = 1; o < 32; o <<= 1) {
+        const int t = __shfl_down_sync(FULLMASK, Q, o);
+        if (lane + o < 32) Q += t;
+    }
+    int x = on ? hb - (Q - pu) : NEG_INF;
+#pragma unroll
+    for (int o = 1; o < 32; o <<= 1) {
+        const int t = __shfl_down_sync(FULLMASK, x, o);
+        if (lane + o < 32) x = max(x, t);
+    }
+    return Q + x;
+}
+
+// the bound-side arrays of the scratch from the path registers (what
+// partial_schedule computes from the job lists)
+__device__ __forceinline__ void partial_from_path(const CtaTables& T, const WarpScratch& S, int f, int b, int hf,
+                                                  int hb, int hr)
+{
+    const int lane = lane_id();
+    if (lane < T.m) {
+        const int fb = (f == 0) ? T.min_arr[lane] : hf;
+        const int bb = (b == 0) ? T.min_dep[lane] : hb;
+        S.frontZ[lane] = hf;
+        S.backZ[lane] = hb;
+        S.Fb[lane] = fb;
+        S.Bb[lane] = bb;
+        S.rem[lane] = hr;
+        S.RB[lane] = hr + bb;
+        S.FR[lane] = fb + hr;
+    }
+    __syncwarp();
+}
+
 // weak node LB (bound_fsp_weak.cpp:289-311), read by every lane
 __device__ __forceinline__ int weak_node_lb(const CtaTables& T, const WarpScratch& S)
 {
@@ -666,7 +738,7 @@ struct NodeCounters {
 template <int NW>
 __device__ __forceinline__ int bound_and_prune(const CtaTables& T, const WarpScratch& S, const DevSearch& srch,
                                                int mode, int (&row)[NW], int k, int f, int b, int line,
-                                               int prev_dir, int best, NodeCounters& cnt)
+                                               int prev_dir, int best, NodeCounters& cnt, bool partial_ready = false)
 {
     const int lane = lane_id();
     bool valid[NW];
@@ -676,7 +748,7 @@ __device__ __forceinline__ int bound_and_prune(const CtaTables& T, const WarpScr
     for (int w = 0; w < NW; w++)
         if (valid[w]) S.rowj[w * 32 + lane] = (unsigned char)row[w];
     __syncwarp();
-    partial_schedule(T, S, f, b, k);
+    if (!partial_ready) partial_schedule(T, S, f, b, k);
 
     const bool both = srch.branch_mode > 0;
     const bool fa = srch.find_all != 0;

@@ -113,6 +113,7 @@ struct pbb_engine {
     int nw = 2, warps = 0, ctas = 0, smem = 0, root_smem = 0;
     DeviceInstance di;
     signed char *mat = nullptr, *vec = nullptr, *bestperm = nullptr;
+    int* path = nullptr;   // per explorer and level: heads, tails, free loads
     int *line = nullptr, *state = nullptr, *bestcost = nullptr, *qval = nullptr, *ub_d = nullptr, *root_d = nullptr;
     int* ival_d = nullptr;   // [2][64] interval start / end vectors
     unsigned* qseq = nullptr;
@@ -163,7 +164,7 @@ int pbb_engine_destroy(pbb_engine* e)
     cudaSetDevice(e->dev);
     if (e->st) cudaStreamSynchronize(e->st);
     e->di.release();
-    cudaFree(e->mat); cudaFree(e->vec); cudaFree(e->bestperm);
+    cudaFree(e->mat); cudaFree(e->vec); cudaFree(e->bestperm); cudaFree(e->path);
     cudaFree(e->line); cudaFree(e->state); cudaFree(e->bestcost); cudaFree(e->qval); cudaFree(e->qseq);
     cudaFree(e->ub_d); cudaFree(e->root_d); cudaFree(e->ival_d); cudaFree(e->ctl); cudaFree(e->group_d);
     cudaFree(e->ngroups_d);
@@ -200,6 +201,7 @@ static int engine_create(const pbb_instance* inst, const pbb_config* cfg, pbb_en
     const int npad = PBB_MAX_N;
     CK(cudaMalloc(&e->mat, (size_t)B * npad * npad));
     CK(cudaMalloc(&e->vec, (size_t)B * npad * 4));
+    CK(cudaMalloc(&e->path, (size_t)B * npad * PBB_PATH_INTS * sizeof(int)));
     CK(cudaMalloc(&e->bestperm, (size_t)B * npad));
     CK(cudaMalloc(&e->line, sizeof(int) * B));
     CK(cudaMalloc(&e->state, sizeof(int) * B));
@@ -235,6 +237,7 @@ static int engine_create(const pbb_instance* inst, const pbb_config* cfg, pbb_en
     g.ivm.bestperm = e->bestperm;
     g.ivm.qseq = e->qseq;
     g.ivm.qval = e->qval;
+    g.ivm.path = e->path;
     g.ctl = e->ctl;
     g.first_cta = 0;
     g.ctas = e->ctas;
@@ -328,7 +331,6 @@ int pbb_explore(pbb_engine* e, double seconds, int32_t* done)
         CK(pbbl::launch_explore(e->nw, e->group_d, e->ngroups_d, e->ctas, e->warps, e->smem, budget, INT_MAX,
                                 e->select_budget, e->st));
         CK(cudaEventRecord(e->ev1, e->st));
-        CK(pbbl::launch_requeue(e->group_d, e->ngroups_d, 1, e->st));
         CK(cudaStreamSynchronize(e->st));
         float ms = 0.f;
         CK(cudaEventElapsedTime(&ms, e->ev0, e->ev1));

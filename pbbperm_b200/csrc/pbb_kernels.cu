@@ -4,7 +4,6 @@
 //   pbb_root_kernel      root row bounded (weak, uncounted) + initial unfold
 //   pbb_explore_kernel   persistent explorer loop: select/decode/bound/prune
 //                        and work sharing through a device idle queue
-//   pbb_requeue_kernel   between launches: re-arm the idle queue
 //   pbb_bound_kernel     batched children bounds of given nodes (LB parity API)
 #include <cuda_runtime.h>
 #include <stdint.h>
@@ -83,7 +82,53 @@ template <int NW>
 struct Ivm {
     int pos[NW], end[NW], dir[NW], pj[NW], row[NW];
     int line;
+    int hf, hb, hr;   // partial schedule of the node at `line`, lane = machine
 };
+
+__device__ __forceinline__ int* path_level(const DevIvms& V, int id, int l)
+{
+    return V.path + ((size_t)id * V.npad + l) * PBB_PATH_INTS;
+}
+
+template <int NW>
+__device__ __forceinline__ void load_path(const DevIvms& V, int id, int l, Ivm<NW>& R)
+{
+    const int* q = path_level(V, id, l) + lane_id();
+    R.hf = __ldcg(q);
+    R.hb = __ldcg(q + 32);
+    R.hr = __ldcg(q + 64);
+}
+
+template <int NW>
+__device__ __forceinline__ void store_path(const DevIvms& V, int id, int l, const Ivm<NW>& R)
+{
+    int* q = path_level(V, id, l) + lane_id();
+    __stcg(q, R.hf);
+    __stcg(q + 32, R.hb);
+    __stcg(q + 64, R.hr);
+}
+
+// path vectors of level L+1 from those of level L, job u fixed on side dir
+template <int NW>
+__device__ __forceinline__ void path_down(const CtaTables& T, Ivm<NW>& R, int u, int dir)
+{
+    if (dir == 0) R.hf = append_front(T, R.hf, u);
+    else R.hb = prepend_back(T, R.hb, u);
+    if (lane_id() < T.m) R.hr -= T.p[lane_id() * T.n + u];
+}
+
+// jobs fixed in front among the levels above L
+template <int NW>
+__device__ __forceinline__ int front_count(const Ivm<NW>& R, int L)
+{
+    int f = 0;
+#pragma unroll
+    for (int w = 0; w < NW; w++) {
+        const int lv = w * 32 + lane_id();
+        f += __popc(__ballot_sync(FULLMASK, lv < L && R.dir[w] == 0));
+    }
+    return f;
+}
 
 __device__ __forceinline__ signed char* mat_row(const DevIvms& V, int id, int l)
 {
@@ -120,6 +165,7 @@ __device__ __forceinline__ void load_ivm(const DevIvms& V, int id, Ivm<NW>& R)
     }
     R.line = __ldcg(V.line + id);
     load_row<NW>(V, id, R.line, R.row);
+    load_path<NW>(V, id, R.line, R);
 }
 
 template <int NW>
@@ -207,6 +253,7 @@ __device__ __forceinline__ int select_node(const DevGroup& G, const CtaTables& T
                 L--;
                 R.line = L;
                 load_row<NW>(G.ivm, id, L, R.row);
+                load_path<NW>(G.ivm, id, L, R);
                 const int pp = vget<NW>(R.pos, L);
                 if (lane_id() == (pp & 31)) {
 #pragma unroll
@@ -230,6 +277,7 @@ __device__ __forceinline__ int select_node(const DevGroup& G, const CtaTables& T
         C.decomposed++;
         const int u = vget<NW>(R.row, p);
         vset<NW>(R.pj, L, u);
+        path_down<NW>(T, R, u, vget<NW>(R.dir, L));
         int nr[NW];
 #pragma unroll
         for (int w = 0; w < NW; w++) {
@@ -244,20 +292,20 @@ __device__ __forceinline__ int select_node(const DevGroup& G, const CtaTables& T
         R.line = L;
         vset<NW>(R.pos, L, 0);
         vset<NW>(R.dir, L, 0);
+        store_path<NW>(G.ivm, id, L, R);
         if (L == n - 1) {                                 // leaf (ivm_bound.cpp:239-271)
             C.leaves++;
-            int f, b;
-            build_lists<NW>(S, R, L, f, b);
+            const int f0 = front_count<NW>(R, L);
             const int last = vget<NW>(R.row, 0);
-            if (lane_id() == 0) S.rowj[0] = (unsigned char)last;
-            __syncwarp();
-            partial_schedule(T, S, f, b, 1);
+            partial_from_path(T, S, f0, L - f0, R.hf, R.hb, R.hr);
             int cost = 0;
             if (lane_id() == 0) cost = makespan_split(T, S, last, -1);
             cost = __shfl_sync(FULLMASK, cost, 0);
             const bool better = fa ? !(cost > best) : !(cost >= best);
             if (better) {
                 best = cost;
+                int f, b;
+                build_lists<NW>(S, R, L, f, b);
                 record_solution<NW>(G, S, id, f, b, last, cost);
             }
             if (lane_id() == 0) {
@@ -277,11 +325,11 @@ __device__ __forceinline__ void bound_current(const DevGroup& G, const CtaTables
                                               Ivm<NW>& R, int mode, int best, WarpCounters& C)
 {
     const int L = R.line;
-    int f, b;
-    build_lists<NW>(S, R, L, f, b);
+    const int f = front_count<NW>(R, L), b = L - f;
+    partial_from_path(T, S, f, b, R.hf, R.hb, R.hr);
     const int prev = L > 0 ? vget<NW>(R.dir, L - 1) : 0;
     NodeCounters nc = {0, 0, 0, 0, 0};
-    const int d = bound_and_prune<NW>(T, S, G.search, mode, R.row, T.n - L, f, b, L, prev, best, nc);
+    const int d = bound_and_prune<NW>(T, S, G.search, mode, R.row, T.n - L, f, b, L, prev, best, nc, true);
     vset<NW>(R.dir, L, d);
     store_row<NW>(G.ivm, id, L, R.row);
     C.simple += nc.simple;
@@ -366,10 +414,6 @@ __device__ __forceinline__ void try_share(const DevGroup& G, int id, Ivm<NW>& R)
     if (l > lcap) l = lcap;
     const int pl = vget<NW>(R.pos, l), el = vget<NW>(R.end, l);
     if (!(pl < el)) return;
-    int thief = -1;
-    if (lane_id() == 0) thief = queue_pop(G);
-    thief = __shfl_sync(FULLMASK, thief, 0);
-    if (thief < 0) return;
 
     int row[NW];
     if (l == R.line) {
@@ -387,6 +431,23 @@ __device__ __forceinline__ void try_share(const DevGroup& G, int id, Ivm<NW>& R)
         em[w] = __ballot_sync(FULLMASK, idx > pl && idx <= el && row[w] >= 0);
         expl += __popc(em[w]);
     }
+    // nothing explorable after pos[l]: a receiver would only skip pruned
+    // cells.  Instead the donor drops those cells from its own interval
+    // (end[l] = pos[l], levels below l open to their last cell), which removes
+    // no node that could be decomposed and lets the next split look deeper.
+    if (expl == 0) {
+#pragma unroll
+        for (int w = 0; w < NW; w++) {
+            const int lv = w * 32 + lane_id();
+            if (lv == l) R.end[w] = pl;
+            else if (lv > l) R.end[w] = n - 1 - lv;
+        }
+        return;
+    }
+    int thief = -1;
+    if (lane_id() == 0) thief = queue_pop(G);
+    thief = __shfl_sync(FULLMASK, thief, 0);
+    if (thief < 0) return;
     const int keep = expl / 2;
     int cut = pl + 1;
     if (keep > 0) {
@@ -410,6 +471,12 @@ __device__ __forceinline__ void try_share(const DevGroup& G, int id, Ivm<NW>& R)
     int* dst = reinterpret_cast<int*>(mat_row(G.ivm, thief, 0));
     const int words = (l + 1) * G.ivm.npad / 4;
     for (int i = lane_id(); i < words; i += 32) __stcg(dst + i, __ldcg(src + i));
+    {
+        const int* ps = path_level(G.ivm, id, 0);
+        int* pd = path_level(G.ivm, thief, 0);
+        const int pw = (l + 1) * PBB_PATH_INTS;
+        for (int i = lane_id(); i < pw; i += 32) __stcg(pd + i, __ldcg(ps + i));
+    }
 #pragma unroll
     for (int w = 0; w < NW; w++) {
         const int lv = w * 32 + lane_id();
@@ -526,6 +593,13 @@ __global__ void pbb_root_kernel(const DevGroup* groups, int ngroups, const int* 
         vset<NW>(R.dir, 0, d);
     }
     store_row<NW>(G.ivm, id, 0, R.row);
+    // path level 0: nothing fixed, every job free
+    R.hf = 0;
+    R.hb = 0;
+    R.hr = 0;
+    if (lane_id() < T.m)
+        for (int j = 0; j < n; j++) R.hr += T.p[lane_id() * n + j];
+    store_path<NW>(G.ivm, id, 0, R);
     NodeCounters nc = {0, 0, 0, 0, 0};
     const int mode = G.search.bound_mode;
     while (R.line < n - 2) {
@@ -533,6 +607,7 @@ __global__ void pbb_root_kernel(const DevGroup* groups, int ngroups, const int* 
         const int p = vget<NW>(R.pos, L);
         if (vget<NW>(R.row, p) < 0) break;             // pos below L are already 0
         vset<NW>(R.pj, L, vget<NW>(R.row, p));
+        path_down<NW>(T, R, vget<NW>(R.row, p), vget<NW>(R.dir, L));
         int nr[NW];
 #pragma unroll
         for (int w = 0; w < NW; w++) {
@@ -544,10 +619,12 @@ __global__ void pbb_root_kernel(const DevGroup* groups, int ngroups, const int* 
 #pragma unroll
         for (int w = 0; w < NW; w++) R.row[w] = nr[w];
         R.line = L + 1;
-        int f, b;
-        build_lists<NW>(S, R, R.line, f, b);
+        store_path<NW>(G.ivm, id, R.line, R);
+        const int f = front_count<NW>(R, R.line), b = R.line - f;
+        partial_from_path(T, S, f, b, R.hf, R.hb, R.hr);
         const int prev = vget<NW>(R.dir, L);
-        const int d = bound_and_prune<NW>(T, S, G.search, mode, R.row, n - R.line, f, b, R.line, prev, best, nc);
+        const int d = bound_and_prune<NW>(T, S, G.search, mode, R.row, n - R.line, f, b, R.line, prev, best, nc,
+                                          true);
         vset<NW>(R.dir, R.line, d);
         store_row<NW>(G.ivm, id, R.line, R.row);
     }
@@ -661,21 +738,6 @@ pbb_explore_kernel(const DevGroup* groups, const int* ngroups_d, int warps_per_c
 __global__ void pbb_lower_ub_kernel(const DevGroup* groups, int g, int ub)
 {
     atomicMin(&groups[g].ctl->best_key, ((unsigned long long)(unsigned)ub << 32) | 0xffffffffull);
-}
-
-// Between two launches: explorers waiting in the queue become idle again and
-// the queue is emptied (the next launch re-registers them).
-__global__ void pbb_requeue_kernel(const DevGroup* groups, const int* ngroups_d)
-{
-    const int ngroups = *ngroups_d;
-    for (int g = blockIdx.y; g < ngroups; g += gridDim.y) {
-        const DevGroup G = groups[g];
-        for (int id = blockIdx.x * blockDim.x + threadIdx.x; id < G.ivm.count; id += gridDim.x * blockDim.x) {
-            if (G.ivm.state[id] != IVM_ACTIVE) G.ivm.state[id] = IVM_IDLE;
-            G.ivm.qseq[id] = (unsigned)id;
-        }
-        if (blockIdx.x == 0 && threadIdx.x == 0) { G.ctl->q_head = 0; G.ctl->q_tail = 0; }
-    }
 }
 
 // Children bounds of `count` nodes (warp per node): weak LBs of every free job
@@ -874,13 +936,6 @@ cudaError_t launch_explore(int nw, const DevGroup* groups, const int* ngroups_d,
         pbb_explore_kernel<2><<<ctas, 32 * warps_per_cta, smem, st>>>(groups, ngroups_d, warps_per_cta, budget_ns,
                                                                        max_rounds, select_budget);
     }
-    return cudaGetLastError();
-}
-
-cudaError_t launch_requeue(const DevGroup* groups, const int* ngroups_d, int max_groups, cudaStream_t st)
-{
-    dim3 grid(64, max_groups < 65535 ? max_groups : 65535);
-    pbb_requeue_kernel<<<grid, 256, 0, st>>>(groups, ngroups_d);
     return cudaGetLastError();
 }
 

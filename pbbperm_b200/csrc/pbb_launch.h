@@ -11,7 +11,6 @@ cudaError_t launch_root(int nw, const DevGroup* groups, int ngroups, const int* 
 cudaError_t launch_lower_ub(const DevGroup* groups, int g, int ub, cudaStream_t st);
 cudaError_t launch_explore(int nw, const DevGroup* groups, const int* ngroups_d, int ctas, int warps_per_cta, int smem,
                            unsigned long long budget_ns, int max_rounds, int select_budget, cudaStream_t st);
-cudaError_t launch_requeue(const DevGroup* groups, const int* ngroups_d, int max_groups, cudaStream_t st);
 int explore_ctas_per_sm(int nw, int warps_per_cta, int smem);
 cudaError_t launch_bound(int nw, const DevInstance& I, int count, const int* sched, const int* l1, const int* l2,
                          int* wb, int* we, int* sb, int* se, int* nweak, int* nstrong, unsigned int* status, int ctas,

@@ -129,10 +129,10 @@ extern "C" void pbb_pool_config_default(pbb_pool_config* c)
     c->max_jobs = 32;
     c->max_machines = 20;
     c->warps_per_cta = 8;
-    c->ctas_per_instance = 1;
-    c->explorers_per_warp = 1;
+    c->ctas_per_instance = 0;
+    c->explorers_per_instance = 1024;
     c->window_s = 0.005;
-    c->explorer_bytes = (int64_t)1 << 30;
+    c->explorer_bytes = (int64_t)8 << 30;
 }
 
 extern "C" int pbb_pool_destroy(pbb_pool* P)
@@ -163,6 +163,7 @@ size_t explorer_block_bytes(int E, int npad)
     size_t b = align256((size_t)E * npad * npad);     // mat
     b += 5 * align256((size_t)E * npad);              // pos end dir pj bestperm
     b += 5 * align256((size_t)E * 4);                 // line state bestcost qseq qval
+    b += align256((size_t)E * npad * PBB_PATH_INTS * 4);   // path levels
     return b;
 }
 
@@ -181,7 +182,8 @@ void carve_explorers(unsigned char* base, int E, int npad, DevIvms& V)
     V.state = reinterpret_cast<int*>(base + o); o += align256((size_t)E * 4);
     V.bestcost = reinterpret_cast<int*>(base + o); o += align256((size_t)E * 4);
     V.qseq = reinterpret_cast<unsigned*>(base + o); o += align256((size_t)E * 4);
-    V.qval = reinterpret_cast<int*>(base + o);
+    V.qval = reinterpret_cast<int*>(base + o); o += align256((size_t)E * 4);
+    V.path = reinterpret_cast<int*>(base + o);
 }
 
 int pool_create(const pbb_pool_config* in, pbb_pool* P)
@@ -193,8 +195,8 @@ int pool_create(const pbb_pool_config* in, pbb_pool* P)
         pbb_pool_config d;
         pbb_pool_config_default(&d);
         if (c.warps_per_cta <= 0) c.warps_per_cta = d.warps_per_cta;
-        if (c.ctas_per_instance <= 0) c.ctas_per_instance = d.ctas_per_instance;
-        if (c.explorers_per_warp <= 0) c.explorers_per_warp = d.explorers_per_warp;
+        if (c.ctas_per_instance < 0) c.ctas_per_instance = 0;
+        if (c.explorers_per_instance <= 0) c.explorers_per_instance = d.explorers_per_instance;
         if (c.window_s <= 0) c.window_s = d.window_s;
         if (c.explorer_bytes <= 0) c.explorer_bytes = d.explorer_bytes;
     }
@@ -211,7 +213,7 @@ int pool_create(const pbb_pool_config* in, pbb_pool* P)
     P->npad = 32 * P->nw;
     P->warps = c.warps_per_cta;
     P->cpi = c.ctas_per_instance;
-    P->epw = c.explorers_per_warp;
+    P->epw = c.explorers_per_instance;
     const int Pmax = c.max_machines * (c.max_machines - 1) / 2;
     P->Ppad_max = (Pmax + 31) / 32 * 32;
     P->smem = pbbl::smem_bytes(c.max_jobs, c.max_machines, P->Ppad_max, P->warps);
@@ -222,10 +224,12 @@ int pool_create(const pbb_pool_config* in, pbb_pool* P)
     if (P->smem > optin) return pfail(PBB_E_INVAL, "tables of max_jobs x max_machines do not fit in shared memory");
     const int per_sm = pbbl::explore_ctas_per_sm(P->nw, P->warps, P->smem);
     if (per_sm < 1) return pfail(PBB_E_INVAL, "explorer kernel cannot be resident with this block shape");
-    int capacity = sms * per_sm / P->cpi;
+    // every window launches all the CTAs the GPU holds at once and spreads
+    // them over the resident instances
+    int capacity = sms * per_sm;
     if (capacity < 1) capacity = 1;
+    P->grid = capacity;
     P->max_slots = c.max_resident > 0 ? std::min(c.max_resident, capacity) : capacity;
-    P->grid = P->max_slots * P->cpi;
     // per-slot instance tables
     P->off_je = 0;
     P->off_p = align256(P->off_je + (size_t)c.max_jobs * P->Ppad_max * 8);
@@ -247,7 +251,7 @@ int pool_create(const pbb_pool_config* in, pbb_pool* P)
     PCK(cudaMalloc(&P->roots_d, sizeof(int) * S * PBB_MAX_N), "roots");
     PCK(cudaMalloc(&P->ivals_d, sizeof(int) * S * 2 * PBB_MAX_N), "intervals");
     P->arena_bytes = (size_t)c.explorer_bytes;
-    const int E = P->cpi * P->warps * P->epw;
+    const int E = P->epw;
     if (explorer_block_bytes(E, P->npad) > P->arena_bytes)
         return pfail(PBB_E_INVAL, "explorer_bytes is smaller than one instance's footprint");
     PCK(cudaMalloc(&P->arena, P->arena_bytes), "explorer memory");
@@ -259,7 +263,7 @@ int pool_create(const pbb_pool_config* in, pbb_pool* P)
     PCK(cudaStreamBeginCapture(P->st, cudaStreamCaptureModeRelaxed), "graph capture");
     cudaError_t e1 = pbbl::launch_explore(P->nw, P->groups_d, P->ngroups_d, P->grid, P->warps, P->smem, budget,
                                           INT_MAX, 4096, P->st);
-    cudaError_t e2 = pbbl::launch_requeue(P->groups_d, P->ngroups_d, S, P->st);
+    cudaError_t e2 = cudaSuccess;
     cudaError_t e3 = cudaMemcpyAsync(P->ctl_h, P->ctl, sizeof(GroupCtl) * S, cudaMemcpyDeviceToHost, P->st);
     cudaError_t e4 = cudaStreamEndCapture(P->st, &graph);
     if (e1 || e2 || e3 || e4) {
@@ -328,7 +332,7 @@ namespace {
 // admit queued instances while a slot and explorer memory are free (FIFO)
 int admit(pbb_pool* P, std::vector<int>& admitted)
 {
-    const int E = P->cpi * P->warps * P->epw;
+    const int E = P->epw;
     const size_t bytes = explorer_block_bytes(E, P->npad);
     while (!P->queue.empty()) {
         int s = -1;
@@ -419,11 +423,22 @@ extern "C" int pbb_pool_step(pbb_pool* P, int32_t* resident, int32_t* queued)
     std::vector<int> act_slot;
     for (int s = 0; s < P->max_slots; s++) {
         if (!P->slots[s].used) continue;
-        DevGroup g = P->slots[s].g;
-        g.first_cta = (int)act.size() * P->cpi;
-        g.ctas = P->cpi;
-        act.push_back(g);
+        act.push_back(P->slots[s].g);
         act_slot.push_back(s);
+    }
+    {
+        // all resident CTAs, spread evenly (a lone instance in the tail of a
+        // batch gets the whole GPU), capped by ctas_per_instance when set
+        const int na = (int)act.size();
+        int first = 0;
+        for (int i = 0; i < na; i++) {
+            int c = P->grid / std::max(1, na) + (i < P->grid % std::max(1, na) ? 1 : 0);
+            if (P->cpi > 0 && c > P->cpi) c = P->cpi;
+            if (c < 1) c = 1;
+            act[i].first_cta = first;
+            act[i].ctas = c;
+            first += c;
+        }
     }
     const int nact = (int)act.size();
     if (nact > 0) {

@@ -76,7 +76,10 @@ struct DevIvms {
     signed char* bestperm; // [count][npad]
     unsigned int* qseq;    // [count] Vyukov queue cell sequence numbers
     int* qval;             // [count] queued explorer ids
+    int* path;             // [count][npad levels][3][32] heads / tails / free loads of the path nodes
 };
+
+#define PBB_PATH_INTS 96   // ints per path level: heads, tails, free loads, 32 machines each
 
 struct DevGroup {
     DevInstance inst;

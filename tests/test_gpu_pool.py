@@ -48,7 +48,7 @@ def test_batch_optima_from_infinity(mix):
     insts, ref = mix
     res = pb.batch_solve(insts, config=pb.Config(boundingMode=2),
                          pool_config=pb.PoolConfig(max_jobs=12, max_machines=10, window_s=0.01,
-                                                   explorers_per_warp=2))
+                                                   explorers_per_instance=4096))
     for p, got, r in zip(insts, res, ref):
         assert got["found"] and got["cost"] == r["opt"]
         assert Oracle(p).eval(got["perm"]) == r["opt"]
