@@ -227,23 +227,23 @@ class Engine:
     def kernel_stats(self):
         """Work of the explorer kernels since start, with the INT32 op model
         of the bounds: weak child 5m ops (add/max chain per machine); per
-        Johnson sweep and machine pair, 2 membership tests per position and
-        pass, 5 ops per free job and pass, 9 ops per evaluated child; per
-        directly scanned child and pair, 1 test per position and 4 ops per
-        free job."""
+        Johnson sweep and machine pair, 5 ops per free job and pass (forward,
+        backward), 9 ops per evaluated child; per directly scanned child and
+        pair, 4 ops per free job (add, add, max, add)."""
         w = _Work()
         _check(lib().pbb_work_counters(self._h, ctypes.byref(w)))
         m, n, P = w.n_machines, w.n_jobs, w.machine_pairs
         ops = (5 * m * w.simple_bounds +
-               P * (4 * n * w.johnson_sweeps + 10 * w.sweep_free_jobs + 9 * w.sweep_children) +
-               P * (n * w.direct_children + 4 * w.direct_free_jobs))
+               P * (10 * w.sweep_free_jobs + 9 * w.sweep_children) +
+               P * 4 * w.direct_free_jobs)
         return dict(device_seconds=w.device_seconds, int32_ops=float(ops), decomposed=w.decomposed,
                     simple_bounds=w.simple_bounds, johnson_bounds=w.johnson_bounds,
                     johnson_sweeps=w.johnson_sweeps, sweep_free_jobs=w.sweep_free_jobs,
                     sweep_children=w.sweep_children, direct_children=w.direct_children,
+                    direct_free_jobs=w.direct_free_jobs,
                     explorers=w.explorers, warps=w.warps,
-                    work_model="5m per weak child + P*(4n per sweep + 10 per swept free job + 9 per swept child)"
-                               " + P*(n + 4 per free job) per directly scanned child")
+                    work_model="5m per weak child + P*(10 per swept free job + 9 per swept child)"
+                               " + P*4 per free job of a directly scanned child")
 
     def explore(self, seconds):
         done = ctypes.c_int32(0)

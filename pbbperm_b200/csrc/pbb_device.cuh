@@ -16,6 +16,10 @@
 #define NEG_INF (-(1 << 28))
 // at most this many children are bounded by direct scans instead of sweeps
 #define PBB_DIRECT_MAX 2
+// Loops over machines and over free jobs stay rolled: the explorer kernel is
+// large and instruction-fetch bound, and unrolled copies of these loops cost
+// more in fetch stalls than they save in loop overhead.
+#define PBB_ROLLED _Pragma("unroll 1")
 
 namespace pbb {
 
@@ -272,6 +276,7 @@ __device__ __forceinline__ int weak_node_lb(const CtaTables& T, const WarpScratc
 {
     int t0 = S.Fb[0] + S.rem[0];
     int lb = t0 + S.Bb[0];
+    PBB_ROLLED
     for (int k = 1; k < T.m; k++) {
         int t1 = max(S.FR[k], t0);
         lb = max(lb, t1 + S.Bb[k]);
@@ -286,6 +291,7 @@ __device__ __forceinline__ int weak_front(const CtaTables& T, const WarpScratch&
     const int n = T.n;
     int t0 = S.Fb[0] + T.p[u];
     int lb = S.Fb[0] + S.RB[0];
+    PBB_ROLLED
     for (int k = 1; k < T.m; k++) {
         int t1 = max(S.Fb[k], t0);
         lb = max(lb, t1 + S.RB[k]);
@@ -300,6 +306,7 @@ __device__ __forceinline__ int weak_back(const CtaTables& T, const WarpScratch& 
     const int n = T.n, m = T.m;
     int t0 = S.Bb[m - 1] + T.p[(m - 1) * n + u];
     int lb = S.FR[m - 1] + S.Bb[m - 1];
+    PBB_ROLLED
     for (int k = m - 2; k >= 0; k--) {
         int t1 = max(t0, S.Bb[k]);
         lb = max(lb, S.FR[k] + t1);
@@ -314,6 +321,7 @@ __device__ __forceinline__ int makespan_split(const CtaTables& T, const WarpScra
 {
     const int n = T.n;
     int h1 = 0, h2 = 0, best = 0;
+    PBB_ROLLED
     for (int k = 0; k < T.m; k++) {
         h1 = max(h1, S.frontZ[k]) + T.p[k * n + x];
         int h = h1;
@@ -490,54 +498,75 @@ __device__ __forceinline__ void johnson_direct(const CtaTables& T, const WarpScr
 // Johnson positions (for the lane's pair i) holding a free job, as a 64-bit
 // mask built from the inverse Johnson order T.posj: scans then visit only the
 // k free positions instead of all n.
+// Johnson positions of the free jobs (rowj[0..k)) for machine pair i, as a mask
 __device__ __forceinline__ unsigned long long free_positions(const CtaTables& T, const WarpScratch& S, int k, int i)
 {
-    unsigned long long pm = 0ull;
     const unsigned char* col = T.posj + i;
+    unsigned long long pm = 0ull;
+    PBB_ROLLED
     for (int q = 0; q < k; q++) pm |= 1ull << col[S.rowj[q] * T.Ppad];
     return pm;
 }
 
-// johnson_direct over the free positions only (needs T.posj).
+// Scan start of child u on pair (m0, m1): front child = heads of front + u,
+// remaining back as is; back child = heads of front, tails of u + back.
+__device__ __forceinline__ void direct_start(const CtaTables& T, const WarpScratch& S, int u, int side, int m0, int m1,
+                                             int& t0, int& t1, int& B0, int& B1)
+{
+    const int m = T.m;
+    if (side == 0) {
+        t0 = S.frontZ[m0] + S.dF[u * m + m0];
+        t1 = S.frontZ[m1] + S.dF[u * m + m1];
+        B0 = S.Bb[m0];
+        B1 = S.Bb[m1];
+    } else {
+        t0 = S.Fb[m0];
+        t1 = S.Fb[m1];
+        B0 = S.backZ[m0] + S.dB[u * m + m0];
+        B1 = S.backZ[m1] + S.dB[u * m + m1];
+    }
+}
+
+// johnson_direct over the free positions only (needs T.posj), one lane per
+// machine pair: the pair's free-position mask is built once and the scans of
+// the one or two children walk it together, each skipping its own job (by
+// select, so that the loop body has no branch).  With one child the second
+// chain repeats the first and is not stored.
 template <int NW>
 __device__ __forceinline__ void johnson_direct_masked(const CtaTables& T, const WarpScratch& S, int k, int nc,
                                                       const int (&cjob)[4], const int (&cside)[4])
 {
+    static_assert(PBB_DIRECT_MAX <= 2, "direct scans walk at most two children together");
+    if (nc == 0) return;
     const int lane = lane_id();
-    const int m = T.m, P = T.P;
-    const int combos = P * nc;
-    for (int base = 0; base < combos; base += 32) {
-        const int q = base + lane;
-        if (q < combos) {
-            int ci = 0, i = q;
-            while (i >= P) { i -= P; ci++; }
-            int u = cjob[0], side = cside[0];
-#pragma unroll
-            for (int c = 1; c < 4; c++)
-                if (ci == c) { u = cjob[c]; side = cside[c]; }
+    const int P = T.P;
+    const int ux = cjob[0], sx = cside[0];
+    const bool two = nc > 1;
+    const int uy = two ? cjob[1] : cjob[0], sy = two ? cside[1] : cside[0];
+    for (int base = 0; base < P; base += 32) {
+        const int i = base + lane;
+        if (i < P) {
             const int m0 = T.pm0[i], m1 = T.pm1[i];
-            int t0, t1, B0, B1;
-            if (side == 0) {
-                t0 = S.frontZ[m0] + S.dF[u * m + m0];
-                t1 = S.frontZ[m1] + S.dF[u * m + m1];
-                B0 = S.Bb[m0];
-                B1 = S.Bb[m1];
-            } else {
-                t0 = S.Fb[m0];
-                t1 = S.Fb[m1];
-                B0 = S.backZ[m0] + S.dB[u * m + m0];
-                B1 = S.backZ[m1] + S.dB[u * m + m1];
-            }
-            unsigned long long pm = free_positions(T, S, k, i) & ~(1ull << T.posj[u * T.Ppad + i]);
+            int t0x, t1x, B0x, B1x, t0y, t1y, B0y, B1y;
+            direct_start(T, S, ux, sx, m0, m1, t0x, t1x, B0x, B1x);
+            direct_start(T, S, uy, sy, m0, m1, t0y, t1y, B0y, B1y);
+            const int px = T.posj[ux * T.Ppad + i];
+            const int py = T.posj[uy * T.Ppad + i];
+            unsigned long long pm = free_positions(T, S, k, i);
             const unsigned long long* col = T.je + i;
             while (pm) {
                 const int t = __ffsll((long long)pm) - 1;
                 pm &= pm - 1ull;
                 const unsigned long long e = col[t * T.Ppad];
-                t0 += JE_A(e);
-                t1 = max(t1, t0 + JE_C(e)) + JE_B(e);
+                const int a = JE_A(e), bb = JE_B(e), c = JE_C(e);
+                t0x += t != px ? a : 0;
+                t0y += t != py ? a : 0;
+                const int nx = max(t1x, t0x + c) + bb, ny = max(t1y, t0y + c) + bb;
+                t1x = t != px ? nx : t1x;
+                t1y = t != py ? ny : t1y;
             }
-            atomicMax(side ? &S.lbB[u] : &S.lbF[u], max(t1 + B1, t0 + B0));
+            atomicMax(sx ? &S.lbB[ux] : &S.lbF[ux], max(t1x + B1x, t0x + B0x));
+            if (two) atomicMax(sy ? &S.lbB[uy] : &S.lbF[uy], max(t1y + B1y, t0y + B0y));
         }
     }
     __syncwarp();
@@ -546,7 +575,8 @@ __device__ __forceinline__ void johnson_direct_masked(const CtaTables& T, const 
 // johnson_children (forward + backward max-plus sweeps) over the free
 // positions only (needs T.posj); same results, O(P k) instead of O(P n).
 template <int NW>
-__device__ __forceinline__ void johnson_sweep_masked(const CtaTables& T, const WarpScratch& S, int k, bool doF,
+__device__ __forceinline__ void johnson_sweep_masked(const CtaTables& T, const WarpScratch& S, int k,
+                                                     bool doF,
                                                      const unsigned (&sF)[NW], bool doB, const unsigned (&sB)[NW])
 {
     const int lane = lane_id();
@@ -565,10 +595,10 @@ __device__ __forceinline__ void johnson_sweep_masked(const CtaTables& T, const W
             const unsigned long long* col = T.je + i;
             const unsigned long long pm = free_positions(T, S, k, i);
             int Apre = 0, Bpre = 0, PMx = NEG_INF;
-            unsigned long long f = pm;
-            while (f) {
-                const int t = __ffsll((long long)f) - 1;
-                f &= f - 1ull;
+            unsigned long long fwd = pm;
+            while (fwd) {
+                const int t = __ffsll((long long)fwd) - 1;
+                fwd &= fwd - 1ull;
                 const unsigned long long e = col[t * T.Ppad];
                 const int u = JE_JOB(e);
                 const unsigned bit = 1u << (u & 31);
@@ -633,6 +663,7 @@ __device__ __forceinline__ void child_tables(const CtaTables& T, const WarpScrat
                 if ((u >> 5) == q) { fw = sF[q]; bw = sB[q]; }
             if (doF && (fw & bit)) {
                 int h = 0;
+                PBB_ROLLED
                 for (int kk = 0; kk < m; kk++) {
                     const int z = S.frontZ[kk];
                     h = max(h, z) + T.p[kk * n + u];
@@ -641,6 +672,7 @@ __device__ __forceinline__ void child_tables(const CtaTables& T, const WarpScrat
             }
             if (doB && (bw & bit)) {
                 int t = 0;
+                PBB_ROLLED
                 for (int kk = m - 1; kk >= 0; kk--) {
                     const int z = S.backZ[kk];
                     t = max(t, z) + T.p[kk * n + u];

@@ -392,9 +392,9 @@ __device__ int queue_pop(const DevGroup& G)
 // ivm::cuttingPosition multicore/src/ivm.cpp:199-237): the first level l where
 // pos and end differ (not below the current line, not deeper than n-10) is
 // cut so that the donor keeps half of the explorable cells after pos[l]; the
-// receiver gets rows 0..l and the right part, and continues with next()
-// without an uncounted unfold, so decomposed-node counts do not depend on
-// how the work was shared.
+// receiver gets row l, the path vectors of level l and the right part, and
+// continues with next() without an uncounted unfold, so decomposed-node counts
+// do not depend on how the work was shared.
 template <int NW>
 __device__ __forceinline__ void try_share(const DevGroup& G, int id, Ivm<NW>& R)
 {
@@ -465,17 +465,19 @@ __device__ __forceinline__ void try_share(const DevGroup& G, int id, Ivm<NW>& R)
             }
         }
     }
-    // receiver image
+    // receiver image.  Above level l the receiver's pos equals its end, so it
+    // never decomposes a node there: going up to l-1 it only flags the cell
+    // it came from and finds its interval exhausted.  Row l and the path
+    // vectors of level l are therefore all it reads of the donor's stack.
     const size_t tb = (size_t)thief * G.ivm.npad;
-    const int* src = reinterpret_cast<const int*>(mat_row(G.ivm, id, 0));
-    int* dst = reinterpret_cast<int*>(mat_row(G.ivm, thief, 0));
-    const int words = (l + 1) * G.ivm.npad / 4;
-    for (int i = lane_id(); i < words; i += 32) __stcg(dst + i, __ldcg(src + i));
+    store_row<NW>(G.ivm, thief, l, row);
     {
-        const int* ps = path_level(G.ivm, id, 0);
-        int* pd = path_level(G.ivm, thief, 0);
-        const int pw = (l + 1) * PBB_PATH_INTS;
-        for (int i = lane_id(); i < pw; i += 32) __stcg(pd + i, __ldcg(ps + i));
+        const int* ps = path_level(G.ivm, id, l) + lane_id();
+        int* pd = path_level(G.ivm, thief, l) + lane_id();
+        const int a = __ldcg(ps), b = __ldcg(ps + 32), c = __ldcg(ps + 64);
+        __stcg(pd, a);
+        __stcg(pd + 32, b);
+        __stcg(pd + 64, c);
     }
 #pragma unroll
     for (int w = 0; w < NW; w++) {
@@ -676,49 +678,74 @@ pbb_explore_kernel(const DevGroup* groups, const int* ngroups_d, int warps_per_c
     WarpCounters C = {0, 0, 0, 0, 0, 0, 0, 0, 0};
     Ivm<NW> R;
     int cached = -1;                   // explorer whose state is held in registers
-    const bool single = (G.ivm.count <= W);
+    unsigned idle_ns = 500;            // back-off of a warp that found nothing to do
     int best = (int)(ld_volatile_u64(&G.ctl->best_key) >> 32);
 
     for (int round = 0; round < max_rounds; round++) {
         if (ld_volatile_s32(&G.ctl->active) == 0) break;
         if (globaltimer_ns() - t0 > budget_ns) break;
         bool worked = false;
-        for (int id = wid; id < G.ivm.count; id += W) {
-            int st = 0;
-            if (lane_id() == 0) st = ld_acquire(G.ivm.state + id);
-            st = __shfl_sync(FULLMASK, st, 0);
-            if (st == IVM_ACTIVE) {
-                if (cached != id) load_ivm<NW>(G.ivm, id, R);
-                cached = id;
-                const int gb = (int)(ld_volatile_u64(&G.ctl->best_key) >> 32);
-                if (gb < best) best = gb;
-                try_share<NW>(G, id, R);
-                const int r = select_node<NW>(G, T, S, id, R, best, C, select_budget);
-                if (r == 1) bound_current<NW>(G, T, S, id, R, mode, best, C);
-                worked = true;
-                if (r == 0) {
-                    // interval exhausted: leave the pool of busy explorers
-                    __syncwarp();
-                    cached = -1;
-                    if (lane_id() == 0) {
-                        st_release(G.ivm.state + id, IVM_QUEUED);
-                        atomicSub(&G.ctl->active, 1);
-                        if (!queue_push(G, id)) st_release(G.ivm.state + id, IVM_IDLE);
+        bool busy = false;          // an explorer of this warp is active or offered
+        int spare = -1;             // an idle explorer of this warp
+        for (int base = wid; base < G.ivm.count; base += 32 * W) {
+            // the states of up to 32 of this warp's explorers in one load
+            // (lane j: explorer base + jW)
+            const int mine = base + lane_id() * W;
+            const int st_l = mine < G.ivm.count ? ld_volatile_s32(G.ivm.state + mine) : -1;
+            unsigned act = __ballot_sync(FULLMASK, st_l == IVM_ACTIVE);
+            const unsigned idl = __ballot_sync(FULLMASK, st_l == IVM_IDLE);
+            if (act || __any_sync(FULLMASK, st_l == IVM_QUEUED)) busy = true;
+            if (spare < 0 && idl) spare = base + (__ffs(idl) - 1) * W;
+            while (act) {
+                const int id = base + (__ffs(act) - 1) * W;
+                act &= act - 1;
+                int st = 0;
+                if (lane_id() == 0) st = ld_acquire(G.ivm.state + id);   // orders the reads of its image
+                st = __shfl_sync(FULLMASK, st, 0);
+                if (st == IVM_ACTIVE) {
+                    if (cached != id) {
+                        // the registers go back to HBM only when the warp moves
+                        // to another explorer (no other warp reads an active one)
+                        if (cached >= 0) store_ivm<NW>(G.ivm, cached, R);
+                        load_ivm<NW>(G.ivm, id, R);
+                        cached = id;
                     }
-                    __syncwarp();
-                } else if (!single) {
-                    store_ivm<NW>(G.ivm, id, R);
-                    cached = -1;
+                    const int gb = (int)(ld_volatile_u64(&G.ctl->best_key) >> 32);
+                    if (gb < best) best = gb;
+                    try_share<NW>(G, id, R);
+                    const int r = select_node<NW>(G, T, S, id, R, best, C, select_budget);
+                    if (r == 1) bound_current<NW>(G, T, S, id, R, mode, best, C);
+                    worked = true;
+                    if (r == 0) {
+                        // interval exhausted: leave the pool of busy explorers
+                        __syncwarp();
+                        cached = -1;
+                        if (lane_id() == 0) {
+                            st_release(G.ivm.state + id, IVM_IDLE);
+                            atomicSub(&G.ctl->active, 1);
+                        }
+                        __syncwarp();
+                    }
                 }
-            } else if (st == IVM_IDLE) {
-                if (lane_id() == 0) {
-                    st_release(G.ivm.state + id, IVM_QUEUED);
-                    if (!queue_push(G, id)) st_release(G.ivm.state + id, IVM_IDLE);
-                }
-                __syncwarp();
             }
+            __syncwarp();
         }
-        if (!worked) __nanosleep(1000);
+        // A warp with nothing to do offers ONE of its idle explorers to the
+        // donors: work is only split towards warps that would otherwise wait,
+        // never towards a warp that is busy with another explorer.
+        if (!busy && spare >= 0 && lane_id() == 0) {
+            st_release(G.ivm.state + spare, IVM_QUEUED);
+            if (!queue_push(G, spare)) st_release(G.ivm.state + spare, IVM_IDLE);
+        }
+        __syncwarp();
+        // idle warps back off (0.5 us doubling to 32 us): their polling
+        // competes with the working warps for issue slots and L2
+        if (!worked) {
+            __nanosleep(idle_ns);
+            idle_ns = idle_ns < 32000u ? 2 * idle_ns : idle_ns;
+        } else {
+            idle_ns = 500;
+        }
     }
     if (cached >= 0) store_ivm<NW>(G.ivm, cached, R);
     if (lane_id() == 0) {
@@ -842,7 +869,7 @@ __global__ void pbb_bound_kernel(DevInstance I, int count, const int* sched, con
             } else {
                 johnson_children<NW>(T, S, um, false, none, false, none, &nl);
                 if (kids) {
-                    // direct scans, four children at a time (front side, then back side)
+                    // direct scans, two children at a time (front side, then back side)
                     int cjob[4] = {0, 0, 0, 0}, cside[4] = {0, 0, 0, 0};
                     int nc = 0;
                     for (int c = 0; c < 2 * k; c++) {
@@ -851,7 +878,7 @@ __global__ void pbb_bound_kernel(DevInstance I, int count, const int* sched, con
                         for (int q = 0; q < 4; q++)
                             if (nc == q) { cjob[q] = j; cside[q] = c < k ? 0 : 1; }
                         nc++;
-                        if (nc == 4 || c == 2 * k - 1) {
+                        if (nc == PBB_DIRECT_MAX || c == 2 * k - 1) {
                             if (T.posj) johnson_direct_masked<NW>(T, S, k, nc, cjob, cside);
                             else johnson_direct<NW>(T, S, um, nc, cjob, cside);
                             nc = 0;

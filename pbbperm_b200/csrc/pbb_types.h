@@ -4,7 +4,7 @@
 
 #define PBB_MAX_N 64          // jobs per instance (int8 IVM cells, two 32-bit mask words)
 #define PBB_MAX_M 32          // machines per instance (one machine per lane in recurrences)
-#define PBB_WARPS_MAX 24
+#define PBB_WARPS_MAX 20      // explorer warps per CTA (96 registers a thread)
 
 // IVM life cycle (per explorer, in global memory)
 #define IVM_IDLE 0            // no interval
@@ -45,15 +45,18 @@ struct DevSearch {
 };
 
 // Per-group control block (device memory).
+// The fields every warp polls or updates under contention each sit on their
+// own 128-byte line, so that reads of the incumbent and of the active count
+// do not queue behind the idle-queue atomics (and the other way round).
 struct GroupCtl {
-    unsigned long long best_key;   // (cost << 32) | ivm id of the slot holding the permutation
-    int active;                    // explorers holding work
-    int found;                     // leaves that improved (or matched, with findAll) the bound
-    unsigned int status;           // PBB_ST_* bits
-    int pad;
+    alignas(128) unsigned long long best_key;   // (cost << 32) | ivm id of the slot holding the permutation
+    alignas(128) int active;                    // explorers holding work
+    alignas(128) unsigned long long q_head;     // idle-explorer queue cursors
+    alignas(128) unsigned long long q_tail;
+    alignas(128) int found;                     // leaves that improved (or matched, with findAll) the bound
+    unsigned int status;                        // PBB_ST_* bits
     unsigned long long decomposed, johnson_bounds, simple_bounds, leaves, root_simple;
-    unsigned long long q_head, q_tail;   // idle-explorer queue cursors
-    unsigned long long steals;           // intervals handed over
+    unsigned long long steals;                  // intervals handed over
     // work of the Johnson sweeps: nodes swept, free jobs summed over them,
     // children evaluated by them (roofline accounting)
     unsigned long long jsweeps, jfree, jchild;

@@ -63,6 +63,8 @@ def run_batch(count=512, pool_config=None, solo_sample=None, device=0):
 
 
 def serve_stream(rate, seconds, seed=7, pool_config=None, device=0, max_requests=20000):
+    """Serve min(rate x seconds, max_requests) requests (at least 20) of the
+    Poisson stream through one pool; latency = completion - arrival."""
     count = max(20, min(max_requests, int(rate * seconds)))
     arr = poisson_arrivals(seed, rate, count)
     insts = [serving_instance(10000 + i) for i in range(count)]
@@ -94,25 +96,35 @@ def serve_stream(rate, seconds, seed=7, pool_config=None, device=0, max_requests
                 costs={t: r["cost"] for t, (_, r) in lat.items()})
 
 
-def serve_alone(rate, count, seed=7, device=0):
-    """The same stream served one request at a time (FIFO) by the
-    single-instance engine; service starts at max(arrival, previous end)."""
-    arr = poisson_arrivals(seed, rate, count)
+def alone_service(count, device=0):
+    """Solve the first `count` requests of the stream one at a time with the
+    single-instance engine; returns their service times (s) and optima.  The
+    request sequence does not depend on the rate, so one measurement serves
+    every rate of a sweep."""
     insts = [serving_instance(10000 + i) for i in range(count)]
     ubs = [pb.neh(p)[0] + 1 for p in insts]
-    t_free = 0.0
-    lats, costs, service = [], {}, []
+    service, costs = [], {}
     for i in range(count):
         t0 = time.perf_counter()
         r = solo_solve(insts[i], ubs[i], device=device)
-        s = time.perf_counter() - t0
-        service.append(s)
-        begin = max(arr[i], t_free)
-        t_free = begin + s
-        lats.append(t_free - arr[i])
+        service.append(time.perf_counter() - t0)
         costs[i] = r["cost"]
+    return service, costs
+
+
+def alone_fifo(rate, service, seed=7):
+    """Latencies of the stream at `rate` served one request at a time (FIFO)
+    with the measured service times: service starts at max(arrival, previous
+    end)."""
+    count = len(service)
+    arr = poisson_arrivals(seed, rate, count)
+    t_free = 0.0
+    lats = []
+    for i in range(count):
+        begin = max(arr[i], t_free)
+        t_free = begin + service[i]
+        lats.append(t_free - arr[i])
     lats_s = sorted(lats)
-    span = t_free - arr[0]
-    return dict(rate=rate, requests=count, throughput=count / span, mean_service_ms=1e3 * statistics.mean(service),
-                p50_ms=1e3 * lats_s[len(lats_s) // 2], p99_ms=1e3 * lats_s[min(count - 1, int(0.99 * count))],
-                costs=costs)
+    return dict(rate=rate, requests=count, throughput=count / (t_free - arr[0]),
+                capacity=count / sum(service), mean_service_ms=1e3 * statistics.mean(service),
+                p50_ms=1e3 * lats_s[len(lats_s) // 2], p99_ms=1e3 * lats_s[min(count - 1, int(0.99 * count))])
