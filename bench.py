@@ -51,8 +51,10 @@ def parse():
     ap.add_argument("--rates", default="10,100,500,2000")
     ap.add_argument("--serve-seconds", type=float, default=20.0)
     ap.add_argument("--serve-requests", type=int, default=300)
-    ap.add_argument("--solo-sample", type=int, default=64)
+    ap.add_argument("--solo-sample", type=int, default=64, help="serve: requests timed one at a time")
+    ap.add_argument("--batch-solo", type=int, default=0, help="batch: instances solved one at a time (0: all)")
     ap.add_argument("--warps-per-cta", type=int, default=0, help="explorer warps per CTA (0: as many as fit)")
+    ap.add_argument("--pool-window", type=float, default=0.02, help="device time per pool window (batch)")
     return ap.parse_args()
 
 
@@ -339,8 +341,8 @@ def run_batch_bench(args):
     t0 = time.perf_counter()
     pc, trials = autotune.tune_pool(insts, ubs, workloads.SEARCH, max_jobs=20, max_machines=20)
     t_tune = time.perf_counter() - t0
-    pc.window_s = 0.02
-    r = workloads.run_batch(args.batch_count, pool_config=pc, solo_sample=args.solo_sample)
+    pc.window_s = args.pool_window
+    r = workloads.run_batch(args.batch_count, pool_config=pc, solo_sample=args.batch_solo)
     out = {"metric": "batched solve throughput (instances/s)", "value": round(r["batch_inst_per_s"], 2),
            "unit": "instances/s", "n_gpus": 1, "higher_is_better": True,
            "config": {"workload": "batch-%d-uneven-n12-20-m5-10-20-seeds100+" % args.batch_count,

@@ -132,7 +132,7 @@ typedef struct pbb_pool_config {
     int32_t warps_per_cta;       /* block shape: warps per CTA (0 = 8) */
     int32_t ctas_per_instance;   /* cap on the CTAs one instance gets in a window (0 = none); every
                                     window spreads all resident CTAs evenly over the instances */
-    int32_t explorers_per_instance; /* explorers (IVMs) of each instance (0 = 1024) */
+    int32_t explorers_per_instance; /* explorers (IVMs) of each instance (0 = one per warp of the grid) */
     int32_t pad;
     double window_s;             /* device time of one window (0 = 0.005) */
     int64_t explorer_bytes;      /* explorer memory budget (0 = 8 GiB) */

@@ -304,7 +304,7 @@ class PoolConfig:
     """Resident pool shape (include/pbbperm.h pbb_pool_config)."""
 
     def __init__(self, max_jobs=32, max_machines=20, max_resident=0, warps_per_cta=8, ctas_per_instance=0,
-                 explorers_per_instance=1024, window_s=0.005, explorer_bytes=8 << 30, device=0):
+                 explorers_per_instance=0, window_s=0.005, explorer_bytes=8 << 30, device=0):
         self.max_jobs = max_jobs
         self.max_machines = max_machines
         self.max_resident = max_resident

@@ -12,7 +12,7 @@ import pbbperm_b200 as pb
 
 CANDIDATES = {
     "warps_per_cta": (4, 8, 16),
-    "explorers_per_instance": (256, 1024, 4096),
+    "explorers_per_instance": (0, 1024),     # 0: one explorer per warp of the grid
 }
 
 

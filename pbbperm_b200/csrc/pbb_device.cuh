@@ -543,8 +543,10 @@ __device__ __forceinline__ void johnson_direct_masked(const CtaTables& T, const 
     const int ux = cjob[0], sx = cside[0];
     const bool two = nc > 1;
     const int uy = two ? cjob[1] : cjob[0], sy = two ? cside[1] : cside[0];
+    int accx = 0, accy = 0;      // child LBs (positive), maxima over all pairs
     for (int base = 0; base < P; base += 32) {
         const int i = base + lane;
+        int vx = 0, vy = 0;
         if (i < P) {
             const int m0 = T.pm0[i], m1 = T.pm1[i];
             int t0x, t1x, B0x, B1x, t0y, t1y, B0y, B1y;
@@ -565,8 +567,19 @@ __device__ __forceinline__ void johnson_direct_masked(const CtaTables& T, const 
                 t1x = t != px ? nx : t1x;
                 t1y = t != py ? ny : t1y;
             }
-            atomicMax(sx ? &S.lbB[ux] : &S.lbF[ux], max(t1x + B1x, t0x + B0x));
-            if (two) atomicMax(sy ? &S.lbB[uy] : &S.lbF[uy], max(t1y + B1y, t0y + B0y));
+            vx = max(t1x + B1x, t0x + B0x);
+            vy = max(t1y + B1y, t0y + B0y);
+        }
+        // one warp reduction per pass instead of 32 colliding shared atomics
+        accx = max(accx, __reduce_max_sync(FULLMASK, vx));
+        accy = max(accy, __reduce_max_sync(FULLMASK, vy));
+    }
+    if (lane == 0) {
+        int* dx = sx ? &S.lbB[ux] : &S.lbF[ux];
+        *dx = max(*dx, accx);
+        if (two) {
+            int* dy = sy ? &S.lbB[uy] : &S.lbF[uy];
+            *dy = max(*dy, accy);
         }
     }
     __syncwarp();

@@ -54,7 +54,7 @@ __device__ __forceinline__ unsigned long long ld_volatile_u64(const unsigned lon
 __device__ __forceinline__ int ld_volatile_s32(const int* p) { return *reinterpret_cast<const volatile int*>(p); }
 
 // Load the group's instance tables into this CTA's shared memory.
-__device__ void load_tables(const DevInstance& I, unsigned char* smem, const SmemPlan& sp, CtaTables& T)
+__device__ __forceinline__ void load_tables(const DevInstance& I, unsigned char* smem, const SmemPlan& sp, CtaTables& T)
 {
     const int tid = threadIdx.x, nt = blockDim.x;
     unsigned long long* je = reinterpret_cast<unsigned long long*>(smem + sp.je_off);
@@ -396,11 +396,13 @@ __device__ int queue_pop(const DevGroup& G)
 // continues with next() without an uncounted unfold, so decomposed-node counts
 // do not depend on how the work was shared.
 template <int NW>
-__device__ __forceinline__ void try_share(const DevGroup& G, int id, Ivm<NW>& R)
+__device__ __forceinline__ int try_share(const DevGroup& G, int id, Ivm<NW>& R)
 {
     const int n = G.inst.n;
-    // cheap emptiness test of the queue first
-    if (ld_volatile_u64(&G.ctl->q_tail) == ld_volatile_u64(&G.ctl->q_head)) return;
+    // cheap emptiness test of the queue first (one lane reads, all follow)
+    int empty = 0;
+    if (lane_id() == 0) empty = ld_volatile_u64(&G.ctl->q_tail) == ld_volatile_u64(&G.ctl->q_head);
+    if (__shfl_sync(FULLMASK, empty, 0)) return 0;
     int f = n;
 #pragma unroll
     for (int w = NW - 1; w >= 0; w--) {
@@ -413,7 +415,7 @@ __device__ __forceinline__ void try_share(const DevGroup& G, int id, Ivm<NW>& R)
     if (l > R.line) l = R.line;
     if (l > lcap) l = lcap;
     const int pl = vget<NW>(R.pos, l), el = vget<NW>(R.end, l);
-    if (!(pl < el)) return;
+    if (!(pl < el)) return 0;
 
     int row[NW];
     if (l == R.line) {
@@ -442,12 +444,12 @@ __device__ __forceinline__ void try_share(const DevGroup& G, int id, Ivm<NW>& R)
             if (lv == l) R.end[w] = pl;
             else if (lv > l) R.end[w] = n - 1 - lv;
         }
-        return;
+        return 2;
     }
     int thief = -1;
     if (lane_id() == 0) thief = queue_pop(G);
     thief = __shfl_sync(FULLMASK, thief, 0);
-    if (thief < 0) return;
+    if (thief < 0) return 0;
     const int keep = expl / 2;
     int cut = pl + 1;
     if (keep > 0) {
@@ -504,6 +506,7 @@ __device__ __forceinline__ void try_share(const DevGroup& G, int id, Ivm<NW>& R)
         st_release(G.ivm.state + thief, IVM_ACTIVE);
     }
     __syncwarp();
+    return 1;
 }
 
 __device__ __forceinline__ int group_of_cta(const DevGroup* groups, int ngroups)
@@ -679,11 +682,17 @@ pbb_explore_kernel(const DevGroup* groups, const int* ngroups_d, int warps_per_c
     Ivm<NW> R;
     int cached = -1;                   // explorer whose state is held in registers
     unsigned idle_ns = 500;            // back-off of a warp that found nothing to do
-    int best = (int)(ld_volatile_u64(&G.ctl->best_key) >> 32);
+    int best = 0;
+    if (lane_id() == 0) best = (int)(ld_volatile_u64(&G.ctl->best_key) >> 32);
+    best = __shfl_sync(FULLMASK, best, 0);
 
     for (int round = 0; round < max_rounds; round++) {
-        if (ld_volatile_s32(&G.ctl->active) == 0) break;
-        if (globaltimer_ns() - t0 > budget_ns) break;
+        // loop control is decided by lane 0 and broadcast, so that the warp
+        // never splits on values read at slightly different times
+        int stop = 0;
+        if (lane_id() == 0)
+            stop = ld_volatile_s32(&G.ctl->active) == 0 || globaltimer_ns() - t0 > budget_ns;
+        if (__shfl_sync(FULLMASK, stop, 0)) break;
         bool worked = false;
         bool busy = false;          // an explorer of this warp is active or offered
         int spare = -1;             // an idle explorer of this warp
@@ -710,7 +719,9 @@ pbb_explore_kernel(const DevGroup* groups, const int* ngroups_d, int warps_per_c
                         load_ivm<NW>(G.ivm, id, R);
                         cached = id;
                     }
-                    const int gb = (int)(ld_volatile_u64(&G.ctl->best_key) >> 32);
+                    int gb = 0;
+                    if (lane_id() == 0) gb = (int)(ld_volatile_u64(&G.ctl->best_key) >> 32);
+                    gb = __shfl_sync(FULLMASK, gb, 0);
                     if (gb < best) best = gb;
                     try_share<NW>(G, id, R);
                     const int r = select_node<NW>(G, T, S, id, R, best, C, select_budget);

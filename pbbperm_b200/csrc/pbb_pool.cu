@@ -130,7 +130,7 @@ extern "C" void pbb_pool_config_default(pbb_pool_config* c)
     c->max_machines = 20;
     c->warps_per_cta = 8;
     c->ctas_per_instance = 0;
-    c->explorers_per_instance = 1024;
+    c->explorers_per_instance = 0;      // one explorer per warp slot of the grid
     c->window_s = 0.005;
     c->explorer_bytes = (int64_t)8 << 30;
 }
@@ -196,7 +196,7 @@ int pool_create(const pbb_pool_config* in, pbb_pool* P)
         pbb_pool_config_default(&d);
         if (c.warps_per_cta <= 0) c.warps_per_cta = d.warps_per_cta;
         if (c.ctas_per_instance < 0) c.ctas_per_instance = 0;
-        if (c.explorers_per_instance <= 0) c.explorers_per_instance = d.explorers_per_instance;
+        if (c.explorers_per_instance < 0) c.explorers_per_instance = 0;
         if (c.window_s <= 0) c.window_s = d.window_s;
         if (c.explorer_bytes <= 0) c.explorer_bytes = d.explorer_bytes;
     }
@@ -229,6 +229,9 @@ int pool_create(const pbb_pool_config* in, pbb_pool* P)
     int capacity = sms * per_sm;
     if (capacity < 1) capacity = 1;
     P->grid = capacity;
+    // default explorer count: every warp of the grid owns one, so that an
+    // instance left alone at the end of a batch can keep the whole GPU busy
+    if (P->epw <= 0) P->epw = P->grid * P->warps;
     P->max_slots = c.max_resident > 0 ? std::min(c.max_resident, capacity) : capacity;
     // per-slot instance tables
     P->off_je = 0;
