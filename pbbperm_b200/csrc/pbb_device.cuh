@@ -15,7 +15,7 @@
 #define FULLMASK 0xffffffffu
 #define NEG_INF (-(1 << 28))
 // at most this many children are bounded by direct scans instead of sweeps
-#define PBB_DIRECT_MAX 2
+#define PBB_DIRECT_MAX 4
 // Loops over machines and over free jobs stay rolled: the explorer kernel is
 // large and instruction-fetch bound, and unrolled copies of these loops cost
 // more in fetch stalls than they save in loop overhead.
@@ -529,60 +529,76 @@ __device__ __forceinline__ void direct_start(const CtaTables& T, const WarpScrat
 
 // johnson_direct over the free positions only (needs T.posj), one lane per
 // machine pair: the pair's free-position mask is built once and the scans of
-// the one or two children walk it together, each skipping its own job (by
-// select, so that the loop body has no branch).  With one child the second
-// chain repeats the first and is not stored.
-template <int NW>
-__device__ __forceinline__ void johnson_direct_masked(const CtaTables& T, const WarpScratch& S, int k, int nc,
+// up to C children walk it together, each skipping its own job (by select, so
+// that the loop body has no branch).  Chains past the child count repeat the
+// first child and are not stored.  Child maxima over the pairs are taken with
+// one warp reduction per pass.
+template <int C>
+__device__ __forceinline__ void johnson_direct_chains(const CtaTables& T, const WarpScratch& S, int k, int nc,
                                                       const int (&cjob)[4], const int (&cside)[4])
 {
-    static_assert(PBB_DIRECT_MAX <= 2, "direct scans walk at most two children together");
-    if (nc == 0) return;
     const int lane = lane_id();
     const int P = T.P;
-    const int ux = cjob[0], sx = cside[0];
-    const bool two = nc > 1;
-    const int uy = two ? cjob[1] : cjob[0], sy = two ? cside[1] : cside[0];
-    int accx = 0, accy = 0;      // child LBs (positive), maxima over all pairs
+    int u[C], sd[C], acc[C];
+#pragma unroll
+    for (int c = 0; c < C; c++) {
+        u[c] = c < nc ? cjob[c] : cjob[0];
+        sd[c] = c < nc ? cside[c] : cside[0];
+        acc[c] = 0;                    // child LBs are positive
+    }
     for (int base = 0; base < P; base += 32) {
         const int i = base + lane;
-        int vx = 0, vy = 0;
+        int v[C];
+#pragma unroll
+        for (int c = 0; c < C; c++) v[c] = 0;
         if (i < P) {
             const int m0 = T.pm0[i], m1 = T.pm1[i];
-            int t0x, t1x, B0x, B1x, t0y, t1y, B0y, B1y;
-            direct_start(T, S, ux, sx, m0, m1, t0x, t1x, B0x, B1x);
-            direct_start(T, S, uy, sy, m0, m1, t0y, t1y, B0y, B1y);
-            const int px = T.posj[ux * T.Ppad + i];
-            const int py = T.posj[uy * T.Ppad + i];
+            int t0[C], t1[C], B0[C], B1[C], px[C];
+#pragma unroll
+            for (int c = 0; c < C; c++) {
+                direct_start(T, S, u[c], sd[c], m0, m1, t0[c], t1[c], B0[c], B1[c]);
+                px[c] = T.posj[u[c] * T.Ppad + i];
+            }
             unsigned long long pm = free_positions(T, S, k, i);
             const unsigned long long* col = T.je + i;
             while (pm) {
                 const int t = __ffsll((long long)pm) - 1;
                 pm &= pm - 1ull;
                 const unsigned long long e = col[t * T.Ppad];
-                const int a = JE_A(e), bb = JE_B(e), c = JE_C(e);
-                t0x += t != px ? a : 0;
-                t0y += t != py ? a : 0;
-                const int nx = max(t1x, t0x + c) + bb, ny = max(t1y, t0y + c) + bb;
-                t1x = t != px ? nx : t1x;
-                t1y = t != py ? ny : t1y;
+                const int a = JE_A(e), bb = JE_B(e), cc = JE_C(e);
+#pragma unroll
+                for (int c = 0; c < C; c++) {
+                    t0[c] += t != px[c] ? a : 0;
+                    const int nx = max(t1[c], t0[c] + cc) + bb;
+                    t1[c] = t != px[c] ? nx : t1[c];
+                }
             }
-            vx = max(t1x + B1x, t0x + B0x);
-            vy = max(t1y + B1y, t0y + B0y);
+#pragma unroll
+            for (int c = 0; c < C; c++) v[c] = max(t1[c] + B1[c], t0[c] + B0[c]);
         }
-        // one warp reduction per pass instead of 32 colliding shared atomics
-        accx = max(accx, __reduce_max_sync(FULLMASK, vx));
-        accy = max(accy, __reduce_max_sync(FULLMASK, vy));
+#pragma unroll
+        for (int c = 0; c < C; c++) acc[c] = max(acc[c], __reduce_max_sync(FULLMASK, v[c]));
     }
     if (lane == 0) {
-        int* dx = sx ? &S.lbB[ux] : &S.lbF[ux];
-        *dx = max(*dx, accx);
-        if (two) {
-            int* dy = sy ? &S.lbB[uy] : &S.lbF[uy];
-            *dy = max(*dy, accy);
+#pragma unroll
+        for (int c = 0; c < C; c++) {
+            if (c < nc) {
+                int* d = sd[c] ? &S.lbB[u[c]] : &S.lbF[u[c]];
+                *d = max(*d, acc[c]);
+            }
         }
     }
     __syncwarp();
+}
+
+template <int NW>
+__device__ __forceinline__ void johnson_direct_masked(const CtaTables& T, const WarpScratch& S, int k, int nc,
+                                                      const int (&cjob)[4], const int (&cside)[4])
+{
+    static_assert(PBB_DIRECT_MAX <= 4, "direct scans walk at most four children together");
+    if (nc <= 0) return;
+    if (nc <= 2) johnson_direct_chains<2>(T, S, k, nc, cjob, cside);
+    else johnson_direct_chains<4>(T, S, k, nc, cjob, cside);
 }
 
 // johnson_children (forward + backward max-plus sweeps) over the free
