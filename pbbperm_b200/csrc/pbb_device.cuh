@@ -498,13 +498,32 @@ __device__ __forceinline__ void johnson_direct(const CtaTables& T, const WarpScr
 // Johnson positions (for the lane's pair i) holding a free job, as a 64-bit
 // mask built from the inverse Johnson order T.posj: scans then visit only the
 // k free positions instead of all n.
+// Position masks over a pair's Johnson order: 32 bits are enough for rows of
+// one word (n <= 32), and cheaper to walk than 64.
+template <int NW>
+struct PosMask {
+    typedef unsigned long long type;
+};
+template <>
+struct PosMask<1> {
+    typedef unsigned type;
+};
+
+__device__ __forceinline__ int low_pos(unsigned m) { return __ffs(m) - 1; }
+__device__ __forceinline__ int low_pos(unsigned long long m) { return __ffsll((long long)m) - 1; }
+__device__ __forceinline__ int high_pos(unsigned m) { return 31 - __clz(m); }
+__device__ __forceinline__ int high_pos(unsigned long long m) { return 63 - __clzll((long long)m); }
+
 // Johnson positions of the free jobs (rowj[0..k)) for machine pair i, as a mask
-__device__ __forceinline__ unsigned long long free_positions(const CtaTables& T, const WarpScratch& S, int k, int i)
+template <int NW>
+__device__ __forceinline__ typename PosMask<NW>::type free_positions(const CtaTables& T, const WarpScratch& S, int k,
+                                                                     int i)
 {
+    typedef typename PosMask<NW>::type M;
     const unsigned char* col = T.posj + i;
-    unsigned long long pm = 0ull;
+    M pm = 0;
     PBB_ROLLED
-    for (int q = 0; q < k; q++) pm |= 1ull << col[S.rowj[q] * T.Ppad];
+    for (int q = 0; q < k; q++) pm |= (M)1 << col[S.rowj[q] * T.Ppad];
     return pm;
 }
 
@@ -529,14 +548,16 @@ __device__ __forceinline__ void direct_start(const CtaTables& T, const WarpScrat
 
 // johnson_direct over the free positions only (needs T.posj), one lane per
 // machine pair: the pair's free-position mask is built once and the scans of
-// up to C children walk it together, each skipping its own job (by select, so
-// that the loop body has no branch).  Chains past the child count repeat the
-// first child and are not stored.  Child maxima over the pairs are taken with
-// one warp reduction per pass.
-template <int C>
+// up to C children walk it together, each skipping its own job by a select, so
+// that the loop body has no branch (cutting the walk at the own positions
+// instead made the lanes of a warp diverge and ran slower).  Chains past the
+// child count repeat the first child and are not stored.  Child maxima over
+// the pairs are taken with one warp reduction per pass.
+template <int C, int NW>
 __device__ __forceinline__ void johnson_direct_chains(const CtaTables& T, const WarpScratch& S, int k, int nc,
                                                       const int (&cjob)[4], const int (&cside)[4])
 {
+    typedef typename PosMask<NW>::type M;
     const int lane = lane_id();
     const int P = T.P;
     int u[C], sd[C], acc[C];
@@ -559,11 +580,11 @@ __device__ __forceinline__ void johnson_direct_chains(const CtaTables& T, const 
                 direct_start(T, S, u[c], sd[c], m0, m1, t0[c], t1[c], B0[c], B1[c]);
                 px[c] = T.posj[u[c] * T.Ppad + i];
             }
-            unsigned long long pm = free_positions(T, S, k, i);
+            M pm = free_positions<NW>(T, S, k, i);
             const unsigned long long* col = T.je + i;
             while (pm) {
-                const int t = __ffsll((long long)pm) - 1;
-                pm &= pm - 1ull;
+                const int t = low_pos(pm);
+                pm &= pm - 1;
                 const unsigned long long e = col[t * T.Ppad];
                 const int a = JE_A(e), bb = JE_B(e), cc = JE_C(e);
 #pragma unroll
@@ -597,8 +618,8 @@ __device__ __forceinline__ void johnson_direct_masked(const CtaTables& T, const 
 {
     static_assert(PBB_DIRECT_MAX <= 4, "direct scans walk at most four children together");
     if (nc <= 0) return;
-    if (nc <= 2) johnson_direct_chains<2>(T, S, k, nc, cjob, cside);
-    else johnson_direct_chains<4>(T, S, k, nc, cjob, cside);
+    if (nc <= 2) johnson_direct_chains<2, NW>(T, S, k, nc, cjob, cside);
+    else johnson_direct_chains<4, NW>(T, S, k, nc, cjob, cside);
 }
 
 // johnson_children (forward + backward max-plus sweeps) over the free
@@ -622,12 +643,13 @@ __device__ __forceinline__ void johnson_sweep_masked(const CtaTables& T, const W
             const int cB2 = S.Fb[m0] + S.backZ[m1];
             const int cB3 = S.Fb[m0] + Asum + S.backZ[m0];
             const unsigned long long* col = T.je + i;
-            const unsigned long long pm = free_positions(T, S, k, i);
+            typedef typename PosMask<NW>::type M;
+            const M pm = free_positions<NW>(T, S, k, i);
             int Apre = 0, Bpre = 0, PMx = NEG_INF;
-            unsigned long long fwd = pm;
+            M fwd = pm;
             while (fwd) {
-                const int t = __ffsll((long long)fwd) - 1;
-                fwd &= fwd - 1ull;
+                const int t = low_pos(fwd);
+                fwd &= fwd - 1;
                 const unsigned long long e = col[t * T.Ppad];
                 const int u = JE_JOB(e);
                 const unsigned bit = 1u << (u & 31);
@@ -650,10 +672,10 @@ __device__ __forceinline__ void johnson_sweep_masked(const CtaTables& T, const W
                 Bpre += b;
             }
             int Asuf = 0, Bsuf = 0, SMx = NEG_INF;
-            unsigned long long r = pm;
+            M r = pm;
             while (r) {
-                const int t = 63 - __clzll((long long)r);
-                r &= ~(1ull << t);
+                const int t = high_pos(r);
+                r &= ~((M)1 << t);
                 const unsigned long long e = col[t * T.Ppad];
                 const int u = JE_JOB(e);
                 const unsigned bit = 1u << (u & 31);

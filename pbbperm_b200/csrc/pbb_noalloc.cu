@@ -166,9 +166,7 @@ static int na_build_tables(const pbb_instance* inst, int johnson_mode, int& P, i
             na_sort(order, 0, n - 1);
             for (int t = 0; t < n; t++) {
                 const int j = order[t];
-                g_stage.je[t * Ppad + i] = (unsigned long long)j | ((unsigned long long)p[a * n + j] << 8) |
-                                           ((unsigned long long)p[b * n + j] << 24) |
-                                           ((unsigned long long)lag[j] << 40);
+                g_stage.je[t * Ppad + i] = JE_PACK(j, p[a * n + j], p[b * n + j], lag[j]);
             }
             i++;
         }

@@ -140,9 +140,7 @@ inline int build_tables(const pbb_instance* inst, int johnson_mode, HostTables& 
         hoare_sort(K, order, 0, n - 1);
         for (int t = 0; t < n; t++) {
             const int j = order[t];
-            const unsigned long long e = (unsigned long long)j | ((unsigned long long)H.p[a * n + j] << 8) |
-                                         ((unsigned long long)H.p[b * n + j] << 24) |
-                                         ((unsigned long long)lag[j] << 40);
+            const unsigned long long e = JE_PACK(j, H.p[a * n + j], H.p[b * n + j], lag[j]);
             H.je[(size_t)t * H.Ppad + i] = e;
             H.posj[(size_t)j * H.Ppad + i] = (unsigned char)t;
         }

@@ -17,10 +17,14 @@
 #define PBB_ST_SPIN 4u
 
 // Packed Johnson entry for (pair i, Johnson position t):
-//   bits 0..7  job id, 8..23 p[m0][job], 24..39 p[m1][job], 40..63 lag[i][job]
-#define JE_JOB(e) ((int)((e) & 0xFFull))
-#define JE_A(e) ((int)(((e) >> 8) & 0xFFFFull))
-#define JE_B(e) ((int)(((e) >> 24) & 0xFFFFull))
+//   bits 0..15 p[m0][job], 16..31 p[m1][job], 32..39 job id, 40..63 lag[i][job]
+// (the two processing times share the low word, so the scans unpack them with
+// one mask and one shift)
+#define JE_PACK(job, a, b, lag) ((unsigned long long)(a) | ((unsigned long long)(b) << 16) | \
+                                 ((unsigned long long)(job) << 32) | ((unsigned long long)(lag) << 40))
+#define JE_A(e) ((int)((unsigned)(e) & 0xFFFFu))
+#define JE_B(e) ((int)((unsigned)(e) >> 16))
+#define JE_JOB(e) ((int)(((e) >> 32) & 0xFFull))
 #define JE_C(e) ((int)((e) >> 40))
 
 // One flow-shop instance as the kernels see it (device pointers).
