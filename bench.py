@@ -347,7 +347,7 @@ def run_batch_bench(args):
     insts = [batch_instance(100 + i) for i in range(args.batch_count)]
     ubs = [pb.neh(p)[0] + 1 for p in insts]
     t0 = time.perf_counter()
-    pc, trials = autotune.tune_pool(insts, ubs, workloads.SEARCH, max_jobs=20, max_machines=20)
+    pc, trials = autotune.tune_pool(insts, ubs, workloads.SEARCH, max_jobs=20, max_machines=20, repeats=2)
     t_tune = time.perf_counter() - t0
     pc.window_s = args.pool_window
     r = workloads.run_batch(args.batch_count, pool_config=pc, solo_sample=args.batch_solo)
