@@ -12,7 +12,10 @@ import pbbperm_b200 as pb
 
 CANDIDATES = {
     "warps_per_cta": (4, 8, 16),
-    "explorers_per_instance": (0, 1024),     # 0: one explorer per warp of the grid
+    # 0: one explorer per warp of the grid, so that an instance left alone at
+    # the end of a batch can still use the whole GPU (a calibration sample
+    # does not show that tail)
+    "explorers_per_instance": (0,),
 }
 
 

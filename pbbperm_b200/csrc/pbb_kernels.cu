@@ -696,50 +696,55 @@ pbb_explore_kernel(const DevGroup* groups, const int* ngroups_d, int warps_per_c
         bool worked = false;
         bool busy = false;          // an explorer of this warp is active or offered
         int spare = -1;             // an idle explorer of this warp
-        for (int base = wid; base < G.ivm.count; base += 32 * W) {
-            // the states of up to 32 of this warp's explorers in one load
-            // (lane j: explorer base + jW)
-            const int mine = base + lane_id() * W;
-            const int st_l = mine < G.ivm.count ? ld_volatile_s32(G.ivm.state + mine) : -1;
-            unsigned act = __ballot_sync(FULLMASK, st_l == IVM_ACTIVE);
-            const unsigned idl = __ballot_sync(FULLMASK, st_l == IVM_IDLE);
-            if (act || __any_sync(FULLMASK, st_l == IVM_QUEUED)) busy = true;
-            if (spare < 0 && idl) spare = base + (__ffs(idl) - 1) * W;
-            while (act) {
-                const int id = base + (__ffs(act) - 1) * W;
-                act &= act - 1;
+        int id = cached;
+        if (id >= 0) {
+            // the explorer held in registers is ACTIVE, and only this warp can
+            // change that: keep stepping it without polling
+            busy = true;
+        } else {
+            for (int base = wid; base < G.ivm.count && id < 0; base += 32 * W) {
+                // the states of up to 32 of this warp's explorers in one load
+                // (lane j: explorer base + jW)
+                const int mine = base + lane_id() * W;
+                const int st_l = mine < G.ivm.count ? ld_volatile_s32(G.ivm.state + mine) : -1;
+                const unsigned act = __ballot_sync(FULLMASK, st_l == IVM_ACTIVE);
+                const unsigned idl = __ballot_sync(FULLMASK, st_l == IVM_IDLE);
+                if (act || __any_sync(FULLMASK, st_l == IVM_QUEUED)) busy = true;
+                if (spare < 0 && idl) spare = base + (__ffs(idl) - 1) * W;
+                if (act) id = base + (__ffs(act) - 1) * W;
+            }
+            if (id >= 0) {
                 int st = 0;
                 if (lane_id() == 0) st = ld_acquire(G.ivm.state + id);   // orders the reads of its image
                 st = __shfl_sync(FULLMASK, st, 0);
                 if (st == IVM_ACTIVE) {
-                    if (cached != id) {
-                        // the registers go back to HBM only when the warp moves
-                        // to another explorer (no other warp reads an active one)
-                        if (cached >= 0) store_ivm<NW>(G.ivm, cached, R);
-                        load_ivm<NW>(G.ivm, id, R);
-                        cached = id;
-                    }
-                    int gb = 0;
-                    if (lane_id() == 0) gb = (int)(ld_volatile_u64(&G.ctl->best_key) >> 32);
-                    gb = __shfl_sync(FULLMASK, gb, 0);
-                    if (gb < best) best = gb;
-                    try_share<NW>(G, id, R);
-                    const int r = select_node<NW>(G, T, S, id, R, best, C, select_budget);
-                    if (r == 1) bound_current<NW>(G, T, S, id, R, mode, best, C);
-                    worked = true;
-                    if (r == 0) {
-                        // interval exhausted: leave the pool of busy explorers
-                        __syncwarp();
-                        cached = -1;
-                        if (lane_id() == 0) {
-                            st_release(G.ivm.state + id, IVM_IDLE);
-                            atomicSub(&G.ctl->active, 1);
-                        }
-                        __syncwarp();
-                    }
+                    load_ivm<NW>(G.ivm, id, R);
+                    cached = id;
+                } else {
+                    id = -1;
                 }
             }
-            __syncwarp();
+        }
+        if (id >= 0) {
+            int gb = 0;
+            if (lane_id() == 0) gb = (int)(ld_volatile_u64(&G.ctl->best_key) >> 32);
+            gb = __shfl_sync(FULLMASK, gb, 0);
+            if (gb < best) best = gb;
+            try_share<NW>(G, id, R);
+            const int r = select_node<NW>(G, T, S, id, R, best, C, select_budget);
+            if (r == 1) bound_current<NW>(G, T, S, id, R, mode, best, C);
+            worked = true;
+            if (r == 0) {
+                // interval exhausted: leave the pool of busy explorers (the
+                // registers need not go back: nobody resumes this interval)
+                __syncwarp();
+                cached = -1;
+                if (lane_id() == 0) {
+                    st_release(G.ivm.state + id, IVM_IDLE);
+                    atomicSub(&G.ctl->active, 1);
+                }
+                __syncwarp();
+            }
         }
         // A warp with nothing to do offers ONE of its idle explorers to the
         // donors: work is only split towards warps that would otherwise wait,

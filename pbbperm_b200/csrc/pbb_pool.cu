@@ -522,7 +522,20 @@ extern "C" int pbb_batch_solve(const pbb_instance* inst, int32_t count, const pb
     pbb_pool* P = nullptr;
     int rc = pbb_pool_create(&c, &P);
     if (rc) return rc;
-    for (int i = 0; i < count && !rc; i++) rc = pbb_pool_submit(P, &inst[i], search, ubs ? ubs[i] : INT32_MAX, nullptr, i);
+    // The whole batch is known: admit the largest instances first (jobs, then
+    // machines), so that the long searches start early and overlap with the
+    // many short ones instead of forming a tail after them.  Results are
+    // matched back by tag, so the order is invisible to the caller.
+    std::vector<int> order(count);
+    for (int i = 0; i < count; i++) order[i] = i;
+    std::stable_sort(order.begin(), order.end(), [&](int a, int b) {
+        if (inst[a].n_jobs != inst[b].n_jobs) return inst[a].n_jobs > inst[b].n_jobs;
+        return inst[a].n_machines > inst[b].n_machines;
+    });
+    for (int q0 = 0; q0 < count && !rc; q0++) {
+        const int i = order[q0];
+        rc = pbb_pool_submit(P, &inst[i], search, ubs ? ubs[i] : INT32_MAX, nullptr, i);
+    }
     int32_t res = 0, q = count;
     std::vector<pbb_pool_result> out(count);
     int got_total = 0;
