@@ -5,20 +5,24 @@
  *
  * Reference interfaces each entry point stands in for (jangmys/PBBPerm):
  *   pbb_engine_create   gpubb::gpubb + initialize + initializeBoundFSP + copyH2D
- *                       (gpu/include/gpubb.h:103-228, gpu/src/gpubb.cu:24-116,
- *                       :826-1060), instance from instance_abstract
+ *                       (gpu/include/gpubb.h:26,151,119,142; gpu/src/gpubb.cu:24-74,
+ *                       83-95, 1004-1062, 917-1003), instance from instance_abstract
  *                       (bounds/include/instance_abstract.h:6-9)
  *   pbb_solve           gpubb::initFullInterval + next + getStats
- *                       (gpubb.h:113,237,245; gpu/src/main.cpp:52-69) and the
- *                       statistics printed by pbab::printStats (common/src/pbab.cpp:40-74)
+ *                       (gpubb.h:36,160,168; gpubb.cu:96,273,1063; gpu/src/main.cpp:52-67)
+ *                       and the statistics printed by pbab::printStats (common/src/pbab.cpp:40-74)
  *   pbb_start / pbb_explore / pbb_get_result
  *                       the same loop in resumable windows (gpubb::next(int&,int&),
- *                       gpubb.h:238; matrix_controller::interruptExploration
+ *                       gpubb.h:161; gpubb::interruptExploration gpubb.h:35;
+ *                       matrix_controller::interruptExploration
  *                       multicore/src/matrix_controller.cpp:459-462)
+ *   pbb_start_interval / pbb_init_from_fac / pbb_get_intervals
+ *                       gpubb::initAtInterval / initFromFac / getIntervals
+ *                       (gpubb.h:155,171,172; gpubb.cu:1190-1310)
  *   pbb_bound_children  bound_abstract::boundChildren + bornes_calculer
  *                       (bounds/include/bound_abstract.h:15-26) for a batch of nodes
  *   pbb_neh             fastNEH::runNEH initial upper bound (heuristic/src/fastNEH.cpp:230-243)
- *   pbb_engine_destroy  gpubb::~gpubb (gpubb.h:104)
+ *   pbb_engine_destroy  gpubb::~gpubb (gpubb.h:27; gpubb.cu:75)
  */
 #ifndef PBBPERM_H
 #define PBBPERM_H
@@ -101,12 +105,30 @@ int pbb_start(pbb_engine* e, int32_t ub, const int32_t* root_perm);
 int pbb_explore(pbb_engine* e, double seconds, int32_t* done);
 
 /* Start on the factoradic interval [pos, end] (n digits each, digit i in
- * [0, n-i)): gpubb::initAtInterval / initFromFac (gpu/include/gpubb.h:232,248),
+ * [0, n-i)): gpubb::initAtInterval (gpu/include/gpubb.h:155),
  * sequentialbb::initAtInterval (multicore/src/sequentialbb.cpp:84-106). */
 int pbb_start_interval(pbb_engine* e, int32_t ub, const int32_t* root_perm, const int32_t* pos, const int32_t* end);
 
+/* Start several explorers at once: interval k ([pos + k*n, end + k*n]) goes
+ * to explorer ids[k] (ids NULL: explorer k); every explorer bounds the root
+ * and unfolds its own start without counting, as initAtInterval does.
+ * Replaces gpubb::initFromFac (gpu/include/gpubb.h:171, gpu/src/gpubb.cu:1245-1310)
+ * and matrix_controller::initFromFac (multicore/include/matrix_controller.h:47).
+ * nb_intervals in [1, nb_ivms]; ids distinct and < nb_ivms. */
+int pbb_init_from_fac(pbb_engine* e, int32_t ub, const int32_t* root_perm, int32_t nb_intervals, const int32_t* ids,
+                      const int32_t* pos, const int32_t* end);
+
+/* Between windows (after pbb_explore returned): the intervals of the
+ * explorers that still hold work, n digits each, with their explorer ids --
+ * a checkpoint that pbb_init_from_fac resumes, in this engine or another.
+ * Replaces gpubb::getIntervals (gpu/include/gpubb.h:172, gpu/src/gpubb.cu:1190-1242),
+ * which also reports explorers by id.  PBB_E_INVAL when max_intervals is too
+ * small (the reference exits there); counters are not reset. */
+int pbb_get_intervals(pbb_engine* e, int32_t max_intervals, int32_t* pos, int32_t* end, int32_t* ids,
+                      int32_t* nb_intervals);
+
 /* Lower the incumbent to `ub` (a bound found by another solver; no
- * permutation is attached): solution::updateCost (common/src/solution.cpp:48-58). */
+ * permutation is attached): solution::updateCost (common/src/solution.cpp:44-56). */
 int pbb_set_ub(pbb_engine* e, int32_t ub);
 int pbb_get_result(pbb_engine* e, pbb_result* out);
 

@@ -399,12 +399,12 @@ typedef struct {
 static int flag_neg(int v) { return v < 0 ? v : -v - 1; }    /* misc.h negative() */
 static int flag_abs(int v) { return v >= 0 ? v : -v - 1; }   /* misc.h absolute() */
 
-static int gt_best(const orc_bb *B, int v)                    /* ivm_bound.cpp:748-752 */
+static int gt_best(const orc_bb *B, int v)                    /* ivm_bound.cpp:678-682 */
 {
     return B->cfg.find_all ? v > B->best : v >= B->best;
 }
 
-/* ivm.cpp:194-202 */
+/* ivm.cpp:153-162 */
 static int before_end(const orc_bb *B)
 {
     for (int i = 0; i < B->n; i++) {
@@ -414,7 +414,7 @@ static int before_end(const orc_bb *B)
     return 1;
 }
 
-/* ivm.cpp:157-173: row `l` is row l-1 without the cell at pos[l-1], flags removed */
+/* ivm.cpp:116-133: row `l` is row l-1 without the cell at pos[l-1], flags removed */
 static void generate_line(orc_bb *B, int l, int explore)
 {
     int n = B->n, c = B->pos[l - 1];
@@ -588,7 +588,7 @@ static int bb_next(orc_bb *B)
     int n = B->n;
     while (before_end(B)) {
         int l = B->line;
-        if (B->pos[l] >= n - l) {                             /* goUp ivm.cpp:97-112 */
+        if (B->pos[l] >= n - l) {                             /* goUp ivm.cpp:56-72 */
             if (l > 0) {
                 B->pos[l] = 0;
                 B->line--;
@@ -601,7 +601,7 @@ static int bb_next(orc_bb *B)
         }
         if (B->mat[l * n + B->pos[l]] < 0) { B->pos[l]++; continue; }   /* goRight */
         B->res.decomposed++;
-        B->line++;                                          /* goDown ivm.cpp:114-146 */
+        B->line++;                                          /* goDown ivm.cpp:73-104 */
         generate_line(B, B->line, 1);
         prepare_schedule(B);
         if (B->line == n - 1) { bound_leaf(B); continue; }

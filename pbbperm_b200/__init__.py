@@ -108,6 +108,9 @@ def lib():
                                          _i32p, _i32p, _i32p, _i32p, _i32p, _i32p, _i32p, _i32p, _i32p]
         L.pbb_neh.argtypes = [ctypes.POINTER(_Instance), _i32p, _i32p]
         L.pbb_start_interval.argtypes = [ctypes.c_void_p, ctypes.c_int32, _i32p, _i32p, _i32p]
+        L.pbb_init_from_fac.argtypes = [ctypes.c_void_p, ctypes.c_int32, _i32p, ctypes.c_int32, _i32p, _i32p, _i32p]
+        L.pbb_get_intervals.argtypes = [ctypes.c_void_p, ctypes.c_int32, _i32p, _i32p, _i32p,
+                                        ctypes.POINTER(ctypes.c_int32)]
         L.pbb_set_ub.argtypes = [ctypes.c_void_p, ctypes.c_int32]
         L.pbb_work_counters.argtypes = [ctypes.c_void_p, ctypes.POINTER(_Work)]
         L.pbb_diag_bound_children.argtypes = [ctypes.POINTER(_Instance), ctypes.c_int32, ctypes.c_int32,
@@ -178,7 +181,7 @@ def _result(r):
 
 
 class Engine:
-    """One instance resident on one GPU (gpubb, gpu/include/gpubb.h:101-250)."""
+    """One instance resident on one GPU (class gpubb, gpu/include/gpubb.h:24-173)."""
 
     def __init__(self, p, config=None):
         self.config = config or Config()
@@ -219,6 +222,34 @@ class Engine:
         pos = np.ascontiguousarray(pos, dtype=np.int32)
         end = np.ascontiguousarray(end, dtype=np.int32)
         _check(lib().pbb_start_interval(self._h, int(ub), _ptr(root), _ptr(pos), _ptr(end)))
+
+    def init_from_fac(self, ub, pos, end, ids=None, root=None):
+        """Start explorer ids[k] (k by default) on interval k: pos and end are
+        (count, n) factoradic digit arrays (gpubb::initFromFac)."""
+        root = None if root is None else np.ascontiguousarray(root, dtype=np.int32)
+        pos = np.ascontiguousarray(pos, dtype=np.int32)
+        end = np.ascontiguousarray(end, dtype=np.int32)
+        count = pos.shape[0]
+        if pos.ndim != 2 or end.shape != pos.shape:
+            raise ValueError("pos and end must be (count, n) arrays of the same shape")
+        ids = None if ids is None else np.ascontiguousarray(ids, dtype=np.int32)
+        _check(lib().pbb_init_from_fac(self._h, int(ub), _ptr(root), int(count), _ptr(ids), _ptr(pos), _ptr(end)))
+
+    def get_intervals(self):
+        """(pos, end, ids) of the explorers still holding work, between windows
+        (gpubb::getIntervals); pos and end are (count, n) arrays."""
+        n = self.n
+        cnt = ctypes.c_int32(0)
+        rc = lib().pbb_get_intervals(self._h, 0, None, None, None, ctypes.byref(cnt))
+        if rc != 0 and cnt.value == 0:
+            _check(rc)
+        k = max(1, cnt.value)
+        pos = np.zeros((k, n), np.int32)
+        end = np.zeros((k, n), np.int32)
+        ids = np.zeros(k, np.int32)
+        _check(lib().pbb_get_intervals(self._h, k, _ptr(pos), _ptr(end), _ptr(ids), ctypes.byref(cnt)))
+        c = cnt.value
+        return pos[:c], end[:c], ids[:c]
 
     def set_ub(self, ub):
         """Lower the incumbent to a bound found elsewhere (no permutation)."""

@@ -65,7 +65,7 @@ __device__ __forceinline__ void vset(int (&x)[NW], int idx, int val)
     }
 }
 
-// ivm.cpp:194-202 -- lexicographic pos <= end over the n levels
+// ivm.cpp:153-162 -- lexicographic pos <= end over the n levels
 template <int NW>
 __device__ __forceinline__ bool before_end(const int (&pos)[NW], const int (&end)[NW], int n)
 {

@@ -310,6 +310,114 @@ int pbb_start_interval(pbb_engine* e, int32_t ub, const int32_t* root_perm, cons
     return start_impl(e, ub, root_perm, pos, end);
 }
 
+int pbb_init_from_fac(pbb_engine* e, int32_t ub, const int32_t* root_perm, int32_t nb_intervals, const int32_t* ids,
+                      const int32_t* pos, const int32_t* end)
+{
+    if (!e) return fail(PBB_E_INVAL, "engine is NULL");
+    if (!pos || !end) return fail(PBB_E_INVAL, "pos/end are NULL");
+    const int B = e->cfg.nb_ivms;
+    if (nb_intervals < 1 || nb_intervals > B) return fail(PBB_E_INVAL, "nb_intervals must be in [1, nb_ivms]");
+    if (ub < 0) return fail(PBB_E_INVAL, "ub must be >= 0");
+    CK(cudaSetDevice(e->dev));
+    const int n = e->H.n;
+    std::vector<int> root(PBB_MAX_N, 0);
+    std::vector<int> seen(n, 0);
+    for (int i = 0; i < n; i++) {
+        const int j = root_perm ? root_perm[i] : i;
+        if (j < 0 || j >= n || seen[j]) return fail(PBB_E_INVAL, "root_perm is not a permutation of 0..n-1");
+        seen[j] = 1;
+        root[i] = j;
+    }
+    std::vector<int> iv((size_t)2 * nb_intervals * PBB_MAX_N, 0);
+    std::vector<int> id(nb_intervals);
+    std::vector<char> taken(B, 0);
+    for (int k = 0; k < nb_intervals; k++) {
+        const int x = ids ? ids[k] : k;
+        if (x < 0 || x >= B || taken[x]) return fail(PBB_E_INVAL, "ids must be distinct explorers < nb_ivms");
+        taken[x] = 1;
+        id[k] = x;
+        for (int i = 0; i < n; i++) {
+            const int p = pos[(size_t)k * n + i], q = end[(size_t)k * n + i];
+            if (p < 0 || p >= n - i || q < 0 || q >= n - i) return fail(PBB_E_INVAL, "interval digit out of range");
+            iv[(size_t)(2 * k) * PBB_MAX_N + i] = p;
+            iv[(size_t)(2 * k + 1) * PBB_MAX_N + i] = q;
+        }
+    }
+    int* ival_d = nullptr;
+    int* ids_d = nullptr;
+    CK(cudaMalloc(&ival_d, sizeof(int) * iv.size()));
+    cudaError_t err = cudaMalloc(&ids_d, sizeof(int) * nb_intervals);
+    if (!err) err = cudaMemcpyAsync(ival_d, iv.data(), sizeof(int) * iv.size(), cudaMemcpyHostToDevice, e->st);
+    if (!err) err = cudaMemcpyAsync(ids_d, id.data(), sizeof(int) * nb_intervals, cudaMemcpyHostToDevice, e->st);
+    if (!err) err = cudaMemcpyAsync(e->ub_d, &ub, sizeof(int), cudaMemcpyHostToDevice, e->st);
+    if (!err) err = cudaMemcpyAsync(e->root_d, root.data(), sizeof(int) * PBB_MAX_N, cudaMemcpyHostToDevice, e->st);
+    if (!err) err = pbbl::launch_reset(e->group_d, 1, e->ub_d, e->st);
+    if (!err)
+        err = pbbl::launch_root(e->nw, e->group_d, 1, e->root_d, ival_d, PBB_MAX_N, e->root_smem, e->st,
+                                nb_intervals, ids_d);
+    if (!err) err = cudaStreamSynchronize(e->st);
+    cudaFree(ival_d);
+    cudaFree(ids_d);
+    if (err) return fail(PBB_E_CUDA, std::string("init_from_fac: ") + cudaGetErrorString(err));
+    GroupCtl c;
+    CK(cudaMemcpy(&c, e->ctl, sizeof(c), cudaMemcpyDeviceToHost));
+    e->ub = ub;
+    e->started = true;
+    e->done = (c.active == 0);
+    e->dev_seconds = 0.0;
+    return PBB_OK;
+}
+
+int pbb_get_intervals(pbb_engine* e, int32_t max_intervals, int32_t* pos, int32_t* end, int32_t* ids,
+                      int32_t* nb_intervals)
+{
+    if (!e || !e->started) return fail(PBB_E_INVAL, "engine not started");
+    if (!nb_intervals) return fail(PBB_E_INVAL, "nb_intervals is NULL");
+    CK(cudaSetDevice(e->dev));
+    CK(cudaStreamSynchronize(e->st));
+    const int B = e->cfg.nb_ivms, n = e->H.n;
+    std::vector<int> st(B);
+    std::vector<signed char> ps((size_t)B * PBB_MAX_N), es((size_t)B * PBB_MAX_N);
+    CK(cudaMemcpy(st.data(), e->state, sizeof(int) * B, cudaMemcpyDeviceToHost));
+    CK(cudaMemcpy(ps.data(), e->group.ivm.pos, ps.size(), cudaMemcpyDeviceToHost));
+    CK(cudaMemcpy(es.data(), e->group.ivm.end, es.size(), cudaMemcpyDeviceToHost));
+    // An explorer stopped between selection steps may hold a digit one past
+    // its level's last cell (n - l: "this level is done"); carry it into the
+    // level above (ivm::goUp, multicore/src/ivm.cpp:56-72) so that every
+    // exported digit lies in [0, n - l), and drop intervals the carry empties.
+    std::vector<int> keep;
+    std::vector<int> pv((size_t)B * n), ev((size_t)B * n);
+    for (int k = 0; k < B; k++) {
+        if (st[k] != IVM_ACTIVE) continue;
+        int* a = &pv[(size_t)k * n];
+        int* z = &ev[(size_t)k * n];
+        for (int i = 0; i < n; i++) {
+            a[i] = ps[(size_t)k * PBB_MAX_N + i];
+            z[i] = es[(size_t)k * PBB_MAX_N + i];
+        }
+        for (int l = n - 1; l > 0; l--)
+            if (a[l] >= n - l) { a[l] = 0; a[l - 1]++; }
+        if (a[0] >= n) continue;
+        bool le = true;     // pos <= end, lexicographically
+        for (int l = 0; l < n; l++)
+            if (a[l] != z[l]) { le = a[l] < z[l]; break; }
+        if (le) keep.push_back(k);
+    }
+    const int cnt = (int)keep.size();
+    *nb_intervals = cnt;
+    if (cnt > max_intervals) return fail(PBB_E_INVAL, "buffer too small for the active intervals");
+    if (cnt > 0 && (!pos || !end)) return fail(PBB_E_INVAL, "pos/end are NULL");
+    for (int w = 0; w < cnt; w++) {
+        const int k = keep[w];
+        for (int i = 0; i < n; i++) {
+            pos[(size_t)w * n + i] = pv[(size_t)k * n + i];
+            end[(size_t)w * n + i] = ev[(size_t)k * n + i];
+        }
+        if (ids) ids[w] = k;
+    }
+    return PBB_OK;
+}
+
 int pbb_set_ub(pbb_engine* e, int32_t ub)
 {
     if (!e || !e->started) return fail(PBB_E_INVAL, "engine not started");

@@ -247,7 +247,7 @@ __device__ __forceinline__ int select_node(const DevGroup& G, const CtaTables& T
         int L = R.line;
         const int k = n - L;
         const int p = vget<NW>(R.pos, L);
-        if (p >= k) {                                    // goUp (ivm.cpp:97-112)
+        if (p >= k) {                                    // goUp (ivm.cpp:56-72)
             if (L > 0) {
                 vset<NW>(R.pos, L, 0);
                 L--;
@@ -273,7 +273,7 @@ __device__ __forceinline__ int select_node(const DevGroup& G, const CtaTables& T
             vset<NW>(R.pos, L, c);
             continue;
         }
-        // goDown (ivm.cpp:114-173): the node at (L, p) is decomposed
+        // goDown (ivm.cpp:73-104): the node at (L, p) is decomposed
         C.decomposed++;
         const int u = vget<NW>(R.row, p);
         vset<NW>(R.pj, L, u);
@@ -544,7 +544,7 @@ __global__ void pbb_reset_kernel(const DevGroup* groups, int ngroups, const int*
                 G.ivm.dir[b + e] = 0;
                 G.ivm.pj[b + e] = 0;
             }
-            G.ivm.pos[b] = (signed char)n;   // empty interval (ivm.cpp:70-76)
+            G.ivm.pos[b] = (signed char)n;   // empty interval (ivm.cpp:36-49)
         }
         if (blockIdx.x == 0 && threadIdx.x == 0) {
             GroupCtl* c = G.ctl;
@@ -564,10 +564,13 @@ __global__ void pbb_reset_kernel(const DevGroup* groups, int ngroups, const int*
 // then the uncounted descent along the interval start (unfold :207-264).
 template <int NW>
 __global__ void pbb_root_kernel(const DevGroup* groups, int ngroups, const int* roots, const int* ivals,
-                                int root_stride)
+                                int root_stride, int per_group, const int* ids)
 {
     extern __shared__ __align__(16) unsigned char smem[];
-    const int g = blockIdx.x;
+    // block b starts explorer ids[b] (b % per_group without ids) of group
+    // b / per_group on interval b
+    const int b = blockIdx.x;
+    const int g = b / per_group;
     if (g >= ngroups) return;
     const DevGroup G = groups[g];
     const SmemPlan sp = pbb_smem_plan(G.inst.n, G.inst.m, G.inst.Ppad, 1);
@@ -576,14 +579,14 @@ __global__ void pbb_root_kernel(const DevGroup* groups, int ngroups, const int* 
     __syncthreads();
     const WarpScratch S = warp_scratch(smem + sp.warp_off, T.m);
     const int n = T.n;
-    const int id = 0;
+    const int id = ids ? ids[b] : b % per_group;
     Ivm<NW> R;
 #pragma unroll
     for (int w = 0; w < NW; w++) {
         const int e = w * 32 + lane_id();
-        // interval [pos, end] of the group (initAtInterval sequentialbb.cpp:84-106)
-        R.pos[w] = e < n ? ivals[(2 * g) * root_stride + e] : 0;
-        R.end[w] = e < n ? ivals[(2 * g + 1) * root_stride + e] : 0;
+        // interval [pos, end] of this explorer (initAtInterval sequentialbb.cpp:84-106)
+        R.pos[w] = e < n ? ivals[(2 * b) * root_stride + e] : 0;
+        R.end[w] = e < n ? ivals[(2 * b + 1) * root_stride + e] : 0;
         R.dir[w] = 0;
         R.pj[w] = 0;
         R.row[w] = e < n ? roots[g * root_stride + e] : 0;
@@ -636,17 +639,17 @@ __global__ void pbb_root_kernel(const DevGroup* groups, int ngroups, const int* 
     store_ivm<NW>(G.ivm, id, R);
     const bool alive = before_end<NW>(R.pos, R.end, n);
     if (lane_id() == 0) {
-        G.ctl->simple_bounds += nc.simple;
-        G.ctl->johnson_bounds += nc.johnson;
-        G.ctl->root_simple += rootc.simple;
-        G.ctl->jsweeps += nc.sweeps;
-        G.ctl->jfree += nc.free_jobs;
-        G.ctl->jchild += nc.swept_children;
-        G.ctl->jdirect += nc.direct_children;
-        G.ctl->jdirect_free += nc.direct_free;
+        atomicAdd(&G.ctl->simple_bounds, nc.simple);
+        atomicAdd(&G.ctl->johnson_bounds, nc.johnson);
+        atomicAdd(&G.ctl->root_simple, rootc.simple);
+        atomicAdd(&G.ctl->jsweeps, nc.sweeps);
+        atomicAdd(&G.ctl->jfree, nc.free_jobs);
+        atomicAdd(&G.ctl->jchild, nc.swept_children);
+        atomicAdd(&G.ctl->jdirect, nc.direct_children);
+        atomicAdd(&G.ctl->jdirect_free, nc.direct_free);
         if (alive) {
-            G.ctl->active = 1;
             G.ivm.state[id] = IVM_ACTIVE;
+            atomicAdd(&G.ctl->active, 1);
         }
     }
 }
@@ -949,14 +952,15 @@ cudaError_t launch_reset(const DevGroup* groups, int ngroups, const int* ub, cud
 }
 
 cudaError_t launch_root(int nw, const DevGroup* groups, int ngroups, const int* roots, const int* ivals,
-                        int root_stride, int smem, cudaStream_t st)
+                        int root_stride, int smem, cudaStream_t st, int per_group, const int* ids)
 {
+    const int blocks = ngroups * per_group;
     if (nw == 1) {
         cudaFuncSetAttribute(pbb_root_kernel<1>, cudaFuncAttributeMaxDynamicSharedMemorySize, smem);
-        pbb_root_kernel<1><<<ngroups, 32, smem, st>>>(groups, ngroups, roots, ivals, root_stride);
+        pbb_root_kernel<1><<<blocks, 32, smem, st>>>(groups, ngroups, roots, ivals, root_stride, per_group, ids);
     } else {
         cudaFuncSetAttribute(pbb_root_kernel<2>, cudaFuncAttributeMaxDynamicSharedMemorySize, smem);
-        pbb_root_kernel<2><<<ngroups, 32, smem, st>>>(groups, ngroups, roots, ivals, root_stride);
+        pbb_root_kernel<2><<<blocks, 32, smem, st>>>(groups, ngroups, roots, ivals, root_stride, per_group, ids);
     }
     return cudaGetLastError();
 }

@@ -6,8 +6,10 @@
 namespace pbbl {
 int smem_bytes(int n, int m, int Ppad, int warps);
 cudaError_t launch_reset(const DevGroup* groups, int ngroups, const int* ub, cudaStream_t st);
+// reset must run first; interval b = g * per_group + j starts explorer j of
+// group g, or explorer ids[b] when ids is given (distinct, < the explorer count)
 cudaError_t launch_root(int nw, const DevGroup* groups, int ngroups, const int* roots, const int* ivals,
-                        int root_stride, int smem, cudaStream_t st);
+                        int root_stride, int smem, cudaStream_t st, int per_group = 1, const int* ids = nullptr);
 cudaError_t launch_lower_ub(const DevGroup* groups, int g, int ub, cudaStream_t st);
 cudaError_t launch_explore(int nw, const DevGroup* groups, const int* ngroups_d, int ctas, int warps_per_cta, int smem,
                            unsigned long long budget_ns, int max_rounds, int select_budget, cudaStream_t st);
