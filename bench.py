@@ -33,8 +33,8 @@ N_JOBS, N_MACH, SEED = 50, 20, 2
 NB_IVMS = 65536
 # explorer-kernel DRAM traffic (read + write) per second of window, from
 # `ncu --set full` on this workload (dram__bytes_read.sum + dram__bytes_write.sum
-# = 13.80 MB + 3.29 MB over a 50.1 ms launch)
-NCU_DRAM_BYTES_PER_S = (13.803008e6 + 3.2896e6) / 0.0501198
+# = 13.61 MB + 3.31 MB over a 50.1 ms launch)
+NCU_DRAM_BYTES_PER_S = (13.607936e6 + 3.314944e6) / 0.050112288
 BOUND_MODE, BRANCH_MODE = 2, 3
 METRIC = "decomposed nodes/s (50x20, Johnson LB)"
 
@@ -274,7 +274,7 @@ def run_ours(args):
         achieved = ops / kern["device_seconds"] / 1e9 if kern["device_seconds"] > 0 else 0.0
         roofline = {"bound": "int32", "achieved": round(achieved, 1), "peak": round(peak, 1), "unit": "Gop/s",
                     "frac": round(achieved / peak, 4) if peak else None,
-                    # DRAM bytes of one explorer launch: 17.09 MB in a 50 ms window of one
+                    # DRAM bytes of one explorer launch: 16.9 MB in a 50 ms window of one
                     # ncu capture of this workload, scaled to this window by device time
                     "traffic": round(NCU_DRAM_BYTES_PER_S * args.window),
                     "traffic_unit": "bytes per launch",
