@@ -143,8 +143,8 @@ int pbb_get_result(pbb_engine* e, pbb_result* out);
  * + 384 x row stride) bytes, row stride 32 for n <= 32 jobs, else 64).  Each pbb_pool_step
  * admits what fits, runs one exploration window of `window_s` device seconds
  * over all resident instances (one captured CUDA graph: explorer kernel,
- * queue re-arm, status read-back), and retires the finished ones, whose
- * results pbb_pool_poll returns.
+ * status read-back), and retires the finished ones, whose results
+ * pbb_pool_poll returns.  pbb_batch_solve admits the largest instances first.
  * ------------------------------------------------------------------------ */
 typedef struct pbb_pool_config {
     int32_t device;

@@ -203,7 +203,7 @@ int pool_create(const pbb_pool_config* in, pbb_pool* P)
     if (c.max_jobs < 2 || c.max_jobs > PBB_MAX_JOBS) return pfail(PBB_E_INVAL, "max_jobs must be in [2, 64]");
     if (c.max_machines < 2 || c.max_machines > PBB_MAX_MACHINES)
         return pfail(PBB_E_INVAL, "max_machines must be in [2, 32]");
-    if (c.warps_per_cta > PBB_WARPS_MAX) return pfail(PBB_E_INVAL, "warps_per_cta must be <= 24");
+    if (c.warps_per_cta > PBB_WARPS_MAX) return pfail(PBB_E_INVAL, "warps_per_cta must be <= 20");
     if (c.window_s > 120.0) return pfail(PBB_E_INVAL, "window_s must be <= 120");
     P->cfg = c;
     P->dev = c.device;
@@ -260,7 +260,7 @@ int pool_create(const pbb_pool_config* in, pbb_pool* P)
     PCK(cudaMalloc(&P->arena, P->arena_bytes), "explorer memory");
     P->alloc.init(P->arena_bytes);
     P->slots.assign(S, Slot());
-    // the window: explorer kernel, queue re-arm, control read-back, as one graph
+    // the window: explorer kernel and control read-back, as one graph
     cudaGraph_t graph = nullptr;
     const unsigned long long budget = (unsigned long long)(c.window_s * 1e9);
     PCK(cudaStreamBeginCapture(P->st, cudaStreamCaptureModeRelaxed), "graph capture");
