@@ -60,7 +60,8 @@ typedef struct pbb_config {
     int32_t find_all;           /* [bb] findAll */
     int32_t johnson_mode;       /* [bb] JohnsonMode: 0 all pairs, 1 (k,m), 2 (k,k+1) */
     int32_t early_stop_johnson; /* [bb] earlyStopJohnson: must be 0 */
-    int32_t sorted_dfs;         /* [bb] sortedDFS: must be 0 */
+    int32_t sorted_dfs;         /* [bb] sortedDFS: 0 (reverse the row on a side change) or 1 (sort it
+                                   by the chosen side's bound, ivm_bound.cpp:344-349); 2-4 rejected */
     int32_t nb_ivms;            /* [gpu] nbIVMs: explorers */
     int32_t device;             /* CUDA device ordinal */
     int32_t warps_per_cta;      /* 0 = largest that fits shared memory */

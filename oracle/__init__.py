@@ -34,7 +34,7 @@ def build_oracle(force=False):
 
 class _OrcCfg(ctypes.Structure):
     _fields_ = [("bound_mode", ctypes.c_int), ("branch_mode", ctypes.c_int),
-                ("find_all", ctypes.c_int), ("node_limit", ctypes.c_int64)]
+                ("find_all", ctypes.c_int), ("sort_nodes", ctypes.c_int), ("node_limit", ctypes.c_int64)]
 
 
 class _OrcResult(ctypes.Structure):
@@ -157,8 +157,9 @@ class Oracle:
         c = lib().orc_neh(self._h, _ptr(perm))
         return c, perm
 
-    def solve(self, ub, bound_mode=2, branch_mode=3, find_all=False, root=None, node_limit=0, pos=None, end=None):
-        cfg = _OrcCfg(bound_mode, branch_mode, 1 if find_all else 0, node_limit)
+    def solve(self, ub, bound_mode=2, branch_mode=3, find_all=False, root=None, node_limit=0, pos=None, end=None,
+              sorted_dfs=0):
+        cfg = _OrcCfg(bound_mode, branch_mode, 1 if find_all else 0, int(sorted_dfs), node_limit)
         res = _OrcResult()
         root = np.arange(self.n, dtype=np.int32) if root is None else np.ascontiguousarray(root, dtype=np.int32)
         perm = np.zeros(self.n, np.int32)
@@ -250,7 +251,7 @@ def write_vrf(dirpath, name, p, ub=None):
 
 
 def run_reference_bb(p, ub=None, bound_mode=2, branch_mode=3, threads=0, johnson=True,
-                     time_limit=None, find_all=False, timeout=3600):
+                     time_limit=None, find_all=False, timeout=3600, sorted_dfs=0):
     """Run the reference multicore B&B (oracle/_ref/bb or bbJ) on instance p.
 
     ub=None means UB=+inf.  Returns the parsed stats dict."""
@@ -261,7 +262,7 @@ def run_reference_bb(p, ub=None, bound_mode=2, branch_mode=3, threads=0, johnson
         with open(os.path.join(d, "mcconfig.ini"), "w") as f:
             f.write("[problem]\nproblem = flowshop\ninstance = %s\n" % name)
             f.write("[initial]\nub = %d\n" % (0 if ub is not None else 3))
-            f.write("[bb]\nsingleNode = true\nsortedDFS = 0\nsortingCriterion = -1\n")
+            f.write("[bb]\nsingleNode = true\nsortedDFS = %d\nsortingCriterion = -1\n" % sorted_dfs)
             f.write("boundingMode = %d\nadaptiveBranchingMode = %d\nJohnsonMode = 0\n" % (bound_mode, branch_mode))
             f.write("earlyStopJohnson = false\nfindAll = %s\n" % ("true" if find_all else "false"))
             f.write("[verbose]\nprintSolutions = false\n")

@@ -370,6 +370,7 @@ typedef struct {
     int bound_mode;    /* [bb] boundingMode: 0 weak, 1 strong, 2 weak then strong */
     int branch_mode;   /* [bb] adaptiveBranchingMode: -3,-2,-1,1,2,3 (CPU numbering) */
     int find_all;      /* [bb] findAll */
+    int sort_nodes;    /* [bb] sortedDFS: 0 (row reversal) or 1 (rows sorted by the first cost) */
     int64_t node_limit;/* stop after this many decomposed nodes (<=0: none) */
 } orc_cfg;
 
@@ -509,17 +510,34 @@ static int choose_dir(const orc_bb *B, const int *cb, const int *ce)
     }
 }
 
-/* ivm_bound.cpp:611-646 with sortedDFS = 0 -> eliminateJobs :338-410 */
+/* misc.h:33-48 gnomeSortByKeyInc: stable, swaps neighbours while the left key
+ * is strictly larger */
+static void gnome_sort_by_key(int *arr, const int *key, int from, int to)
+{
+    int i = from + 1, j = i + 1;
+    while (i <= to) {
+        if (key[arr[i - 1]] > key[arr[i]]) {
+            int t = arr[i - 1]; arr[i - 1] = arr[i]; arr[i] = t;
+            if (--i) continue;
+        }
+        i = j++;
+    }
+}
+
+/* ivm_bound.cpp:611-646 -> eliminateJobs :338-410.  sortedDFS = 0 reverses the
+ * row when the side changes; sortedDFS = 1 sorts it by the chosen side's first
+ * cost instead (:344-349). */
 static void prune(orc_bb *B, const int *c1b, const int *c1e, const int *c2b, const int *c2e)
 {
     int n = B->n, l = B->line;
     int *row = B->mat + l * n;
     int prev = l > 0 ? B->dir[l - 1] : 0;
-    if (prev != B->dir[l]) {
+    if (B->cfg.sort_nodes == 0 && prev != B->dir[l]) {
         for (int a = 0, b = n - l - 1; a < b; a++, b--) { int t = row[a]; row[a] = row[b]; row[b] = t; }
     }
     const int *c1 = B->dir[l] == 1 ? c1e : c1b;
     const int *c2 = B->dir[l] == 1 ? c2e : c2b;
+    if (B->cfg.sort_nodes == 1) gnome_sort_by_key(row, c1, 0, n - l - 1);
     for (int i = 0; i < n - l; i++) {
         int j = row[i];
         if (gt_best(B, c1[j]) || gt_best(B, c2[j])) row[i] = flag_neg(j);

@@ -943,8 +943,41 @@ __device__ __forceinline__ int bound_and_prune(const CtaTables& T, const WarpScr
         bool cut = fa ? (c1 > best || c2 > best) : (c1 >= best || c2 >= best);
         if (valid[w] && cut) row[w] = cell_flag(row[w]);
     }
-    // reverse the row when the side changes from the previous level (:620-636)
-    if (prev_dir != dir) {
+    if (srch.sort_nodes) {
+        // sortedDFS = 1: eliminateJobs sorts the row by the chosen side's first
+        // cost (ivm_bound.cpp:344-349) with a stable gnome sort (misc.h:33-48);
+        // a cell's place = cells with a smaller key + earlier cells with the same
+        int key[NW], rank[NW];
+#pragma unroll
+        for (int w = 0; w < NW; w++) {
+            key[w] = (mode == 1) ? (dir ? ces[w] : cbs[w]) : (dir ? cew[w] : cbw[w]);
+            rank[w] = 0;
+        }
+#pragma unroll
+        for (int jw = 0; jw < NW; jw++) {
+            PBB_ROLLED
+            for (int jl = 0; jl < 32; jl++) {
+                const int j = jw * 32 + jl;
+                if (j >= k) break;
+                const int kj = __shfl_sync(FULLMASK, key[jw], jl);
+#pragma unroll
+                for (int w = 0; w < NW; w++) {
+                    const int i = w * 32 + lane;
+                    rank[w] += (kj < key[w] || (kj == key[w] && j < i)) ? 1 : 0;
+                }
+            }
+        }
+        unsigned char* tmp = S.rowj;       // free after the Johnson scans
+#pragma unroll
+        for (int w = 0; w < NW; w++)
+            if (valid[w]) tmp[rank[w]] = (unsigned char)(signed char)row[w];
+        __syncwarp();
+#pragma unroll
+        for (int w = 0; w < NW; w++)
+            if (valid[w]) row[w] = (signed char)tmp[w * 32 + lane];
+        __syncwarp();
+    } else if (prev_dir != dir) {
+        // reverse the row when the side changes from the previous level (:620-636)
         int nr[NW];
 #pragma unroll
         for (int w = 0; w < NW; w++) {

@@ -153,7 +153,8 @@ static int check_config(const pbb_config* c)
     if (!(b == -3 || b == -2 || b == -1 || b == 1 || b == 2 || b == 3))
         return fail(PBB_E_INVAL, "adaptiveBranchingMode must be one of -3,-2,-1,1,2,3");
     if (c->early_stop_johnson) return fail(PBB_E_UNSUPPORTED, "earlyStopJohnson=true is not supported");
-    if (c->sorted_dfs) return fail(PBB_E_UNSUPPORTED, "sortedDFS != 0 is not supported");
+    if (c->sorted_dfs < 0 || c->sorted_dfs > 1)
+        return fail(PBB_E_UNSUPPORTED, "sortedDFS must be 0 or 1 (2-4 sort by idle-time priorities, not computed here)");
     if (c->nb_ivms < 1 || c->nb_ivms > (1 << 22)) return fail(PBB_E_INVAL, "nbIVMs must be in [1, 4194304]");
     return PBB_OK;
 }
@@ -224,6 +225,7 @@ static int engine_create(const pbb_instance* inst, const pbb_config* cfg, pbb_en
     g.search.bound_mode = cfg->bounding_mode;
     g.search.branch_mode = cfg->branching_mode;
     g.search.find_all = cfg->find_all ? 1 : 0;
+    g.search.sort_nodes = cfg->sorted_dfs;
     g.ivm.count = B;
     g.ivm.npad = npad;
     g.ivm.mat = e->mat;

@@ -46,6 +46,7 @@ struct DevSearch {
     int bound_mode;    // 0 weak, 1 strong, 2 weak then strong
     int branch_mode;   // -3,-2,-1 fixed; 1 MaxSum, 2 MinBranch, 3 MinMin
     int find_all;
+    int sort_nodes;    // [bb] sortedDFS: 0 reverse the row on a side change, 1 sort it by cost
 };
 
 // Per-group control block (device memory).

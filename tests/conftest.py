@@ -35,3 +35,8 @@ def bounds_golden():
 @pytest.fixture(scope="session")
 def search_golden():
     return load_golden("search_golden.json")
+
+
+@pytest.fixture(scope="session")
+def sorted_golden():
+    return load_golden("sorted_golden.json")

@@ -13,9 +13,12 @@ B&B `bb` / `bbJ`).  Instances come from the project's seeded generator
   search_golden.json  reference multicore B&B runs with UB = optimum:
                       TOTdecomposed / TOTjohnson LBs / TOTsimple LBs / TOTleaves
                       per (instance, boundingMode, adaptiveBranchingMode, findAll).
+  sorted_golden.json  reference B&B runs on ONE thread from UB = +inf with
+                      sortedDFS 0 and 1: the exploration order decides when the
+                      bound improves, so the counters pin the order of the children.
 
-Usage: python tests/golden/make_golden.py [--big]   (--big adds the 20x20
-seed-1 instance, several CPU-minutes of reference time)
+Usage: python tests/golden/make_golden.py [--big] [--sorted-only]   (--big adds
+the 20x20 seed-1 instance, several CPU-minutes of reference time)
 """
 import json
 import os
@@ -40,6 +43,8 @@ NODES_PER_CASE = 40
 SEARCH_CASES = [(10, 5, 21), (12, 10, 22), (14, 5, 23), (13, 20, 24), (16, 8, 25), (20, 5, 0), (11, 3, 26),
                 (9, 12, 27), (15, 6, 28), (35, 10, 45)]
 TINY_CASES = [(8, 4, 29), (9, 6, 30), (7, 10, 31)]
+SORTED_CASES = [(9, 5, 41), (10, 5, 42), (11, 8, 43), (10, 10, 44)]
+SORTED_MODES = [(0, 3), (2, 3), (2, 1), (1, 2), (2, -3)]
 
 
 def child_strong(R, sched, l1, l2, front):
@@ -152,10 +157,29 @@ def make_search(big=False):
         json.dump(dict(source="reference multicore B&B (oracle/_ref/bb, bbJ), 8 threads", runs=runs), f, indent=0)
 
 
+def make_sorted():
+    runs = []
+    for n, m, seed in SORTED_CASES:
+        p = synthetic_instance(seed, n, m)
+        for bm, br in SORTED_MODES:
+            for sd in (0, 1):
+                r = run_reference_bb(p, ub=None, bound_mode=bm, branch_mode=br, threads=1, johnson=(bm != 0),
+                                     sorted_dfs=sd, timeout=600)
+                runs.append(dict(n=n, m=m, seed=seed, p=p.tolist(), bounding_mode=bm, branching_mode=br,
+                                 sorted_dfs=sd, best=r["best"], decomposed=r["decomposed"],
+                                 johnson_bounds=r["johnson_bounds"], simple_bounds=r["simple_bounds"],
+                                 leaves=r["leaves"]))
+    with open(os.path.join(HERE, "sorted_golden.json"), "w") as f:
+        json.dump(dict(source="reference multicore B&B (oracle/_ref/bb, bbJ), 1 thread, UB = +inf", runs=runs),
+                  f, indent=0)
+
+
 if __name__ == "__main__":
     if not oracle.reference_available():
         sys.exit("build the reference checker first: python oracle/build_ref.py")
-    if "--search-only" not in sys.argv:
-        make_bounds()
-    make_search(big="--big" in sys.argv)
+    if "--sorted-only" not in sys.argv:
+        if "--search-only" not in sys.argv:
+            make_bounds()
+        make_search(big="--big" in sys.argv)
+    make_sorted()
     print("golden fixtures written to", HERE)

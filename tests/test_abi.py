@@ -49,7 +49,7 @@ def test_unsupported_options_rejected():
         pb.Engine(p, pb.Config(earlyStopJohnson=True))
     assert e.value.code == pb.PBB_E_UNSUPPORTED
     with pytest.raises(pb.PbbError) as e:
-        pb.Engine(p, pb.Config(sortedDFS=1))
+        pb.Engine(p, pb.Config(sortedDFS=2))           # sorts by idle-time priorities
     assert e.value.code == pb.PBB_E_UNSUPPORTED
     with pytest.raises(pb.PbbError) as e:
         pb.Engine(p, pb.Config(adaptiveBranchingMode=4))

@@ -18,6 +18,32 @@ def solve(p, ub, ivms=1024, **cfg):
         return e.solve(ub=ub)
 
 
+def test_sorted_dfs_sequential_vs_reference_golden(sorted_golden):
+    """One explorer from UB = +inf explores in the reference's sequential order,
+    so its counters, which depend on when the bound improves, must equal the
+    reference's single-thread run, with the rows reversed (sortedDFS = 0) or
+    sorted by the chosen side's bound (sortedDFS = 1)."""
+    for r in sorted_golden["runs"]:
+        p = np.array(r["p"], np.int32)
+        got = solve(p, 2**31 - 1, ivms=1, boundingMode=r["bounding_mode"],
+                    adaptiveBranchingMode=r["branching_mode"], sortedDFS=r["sorted_dfs"])
+        assert got["complete"] and got["found"] and got["cost"] == r["best"]
+        for k in KEYS:
+            assert got[k] == r[k], (r["seed"], r["bounding_mode"], r["branching_mode"], r["sorted_dfs"], k,
+                                    got[k], r[k])
+
+
+@pytest.mark.parametrize("ivms", [64, 16384])
+def test_sorted_dfs_counters_at_the_optimum(ivms):
+    """At UB = optimum the node set does not depend on the order, with any
+    number of explorers: counters equal the oracle's with the same sort."""
+    p = synthetic_instance(24, 13, 20)
+    want = Oracle(p).solve(1803, bound_mode=2, sorted_dfs=1)
+    got = solve(p, 1803, ivms=ivms, boundingMode=2, sortedDFS=1)
+    for k in KEYS:
+        assert got[k] == want[k], (k, got[k], want[k])
+
+
 def test_counters_vs_reference_golden(search_golden):
     for r in search_golden["runs"]:
         if r.get("ub") is None or r.get("big"):
