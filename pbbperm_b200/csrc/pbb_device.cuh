@@ -817,8 +817,27 @@ struct NodeCounters {
 // back lists already in S.fjob / S.bjob, f and b long), choose the branching
 // side and prune the row in place (ivm_bound.cpp weak/strong/mixedBoundPrune
 // :650-676 -> chooseChildrenSet, prune :611-646 with sortedDFS = 0).
+// Stable sort of a row's k cells (k <= 64; lane l holds cells l and 32 + l) by
+// key, written to out[0..k): a cell's place = cells with a smaller key plus
+// earlier cells with the same key, the order gnomeSortByKeyInc (misc.h:33-48)
+// leaves.  Called by all 32 lanes.
+__device__ __noinline__ void sort_cells(unsigned char* out, int k, int key0, int key1, int cell0, int cell1)
+{
+    const int lane = lane_id();
+    int r0 = 0, r1 = 0;
+    PBB_ROLLED
+    for (int j = 0; j < k; j++) {
+        const int kj = __shfl_sync(FULLMASK, j < 32 ? key0 : key1, j & 31);
+        r0 += (kj < key0 || (kj == key0 && j < lane)) ? 1 : 0;
+        r1 += (kj < key1 || (kj == key1 && j < lane + 32)) ? 1 : 0;
+    }
+    if (lane < k) out[r0] = (unsigned char)(signed char)cell0;
+    if (lane + 32 < k) out[r1] = (unsigned char)(signed char)cell1;
+    __syncwarp();
+}
+
 // Returns the side chosen for this level.
-template <int NW>
+template <int NW, int SORT = 1>
 __device__ __forceinline__ int bound_and_prune(const CtaTables& T, const WarpScratch& S, const DevSearch& srch,
                                                int mode, int (&row)[NW], int k, int f, int b, int line,
                                                int prev_dir, int best, NodeCounters& cnt, bool partial_ready = false)
@@ -943,38 +962,16 @@ __device__ __forceinline__ int bound_and_prune(const CtaTables& T, const WarpScr
         bool cut = fa ? (c1 > best || c2 > best) : (c1 >= best || c2 >= best);
         if (valid[w] && cut) row[w] = cell_flag(row[w]);
     }
-    if (srch.sort_nodes) {
+    if (SORT && srch.sort_nodes) {
         // sortedDFS = 1: eliminateJobs sorts the row by the chosen side's first
-        // cost (ivm_bound.cpp:344-349) with a stable gnome sort (misc.h:33-48);
-        // a cell's place = cells with a smaller key + earlier cells with the same
-        int key[NW], rank[NW];
+        // cost (ivm_bound.cpp:344-349), out of line to keep the hot loop small
+        int key[NW];
 #pragma unroll
-        for (int w = 0; w < NW; w++) {
-            key[w] = (mode == 1) ? (dir ? ces[w] : cbs[w]) : (dir ? cew[w] : cbw[w]);
-            rank[w] = 0;
-        }
-#pragma unroll
-        for (int jw = 0; jw < NW; jw++) {
-            PBB_ROLLED
-            for (int jl = 0; jl < 32; jl++) {
-                const int j = jw * 32 + jl;
-                if (j >= k) break;
-                const int kj = __shfl_sync(FULLMASK, key[jw], jl);
-#pragma unroll
-                for (int w = 0; w < NW; w++) {
-                    const int i = w * 32 + lane;
-                    rank[w] += (kj < key[w] || (kj == key[w] && j < i)) ? 1 : 0;
-                }
-            }
-        }
-        unsigned char* tmp = S.rowj;       // free after the Johnson scans
+        for (int w = 0; w < NW; w++) key[w] = (mode == 1) ? (dir ? ces[w] : cbs[w]) : (dir ? cew[w] : cbw[w]);
+        sort_cells(S.rowj, k, key[0], NW > 1 ? key[NW - 1] : 0, row[0], NW > 1 ? row[NW - 1] : 0);
 #pragma unroll
         for (int w = 0; w < NW; w++)
-            if (valid[w]) tmp[rank[w]] = (unsigned char)(signed char)row[w];
-        __syncwarp();
-#pragma unroll
-        for (int w = 0; w < NW; w++)
-            if (valid[w]) row[w] = (signed char)tmp[w * 32 + lane];
+            if (valid[w]) row[w] = (signed char)S.rowj[w * 32 + lane];
         __syncwarp();
     } else if (prev_dir != dir) {
         // reverse the row when the side changes from the previous level (:620-636)

@@ -439,7 +439,7 @@ int pbb_explore(pbb_engine* e, double seconds, int32_t* done)
         const unsigned long long budget = (unsigned long long)(win * 1e9);
         CK(cudaEventRecord(e->ev0, e->st));
         CK(pbbl::launch_explore(e->nw, e->group_d, e->ngroups_d, e->ctas, e->warps, e->smem, budget, INT_MAX,
-                                e->select_budget, e->st));
+                                e->select_budget, e->st, e->cfg.sorted_dfs));
         CK(cudaEventRecord(e->ev1, e->st));
         CK(cudaStreamSynchronize(e->st));
         float ms = 0.f;

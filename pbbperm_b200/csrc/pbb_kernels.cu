@@ -320,7 +320,7 @@ __device__ __forceinline__ int select_node(const DevGroup& G, const CtaTables& T
 }
 
 // Bound and prune the node selected at R.line and write its row back.
-template <int NW>
+template <int NW, int SORT>
 __device__ __forceinline__ void bound_current(const DevGroup& G, const CtaTables& T, const WarpScratch& S, int id,
                                               Ivm<NW>& R, int mode, int best, WarpCounters& C)
 {
@@ -329,7 +329,7 @@ __device__ __forceinline__ void bound_current(const DevGroup& G, const CtaTables
     partial_from_path(T, S, f, b, R.hf, R.hb, R.hr);
     const int prev = L > 0 ? vget<NW>(R.dir, L - 1) : 0;
     NodeCounters nc = {0, 0, 0, 0, 0};
-    const int d = bound_and_prune<NW>(T, S, G.search, mode, R.row, T.n - L, f, b, L, prev, best, nc, true);
+    const int d = bound_and_prune<NW, SORT>(T, S, G.search, mode, R.row, T.n - L, f, b, L, prev, best, nc, true);
     vset<NW>(R.dir, L, d);
     store_row<NW>(G.ivm, id, L, R.row);
     C.simple += nc.simple;
@@ -656,8 +656,10 @@ __global__ void pbb_root_kernel(const DevGroup* groups, int ngroups, const int* 
 
 // Persistent explorer loop.  Warp w of a group serves explorers w, w+W, ...
 // (W = warps of the group).  Runs until no explorer of the group holds work,
-// or `budget_ns` of device time has passed, or `max_rounds` rounds.
-template <int NW>
+// or `budget_ns` of device time has passed, or `max_rounds` rounds.  SORT = 0
+// compiles the sortedDFS row sort out of the hot loop (SORT = 1 follows each
+// group's setting).
+template <int NW, int SORT>
 __global__ void __launch_bounds__(32 * PBB_WARPS_MAX, 1)
 pbb_explore_kernel(const DevGroup* groups, const int* ngroups_d, int warps_per_cta, unsigned long long budget_ns,
                    int max_rounds, int select_budget)
@@ -735,7 +737,7 @@ pbb_explore_kernel(const DevGroup* groups, const int* ngroups_d, int warps_per_c
             if (gb < best) best = gb;
             try_share<NW>(G, id, R);
             const int r = select_node<NW>(G, T, S, id, R, best, C, select_budget);
-            if (r == 1) bound_current<NW>(G, T, S, id, R, mode, best, C);
+            if (r == 1) bound_current<NW, SORT>(G, T, S, id, R, mode, best, C);
             worked = true;
             if (r == 0) {
                 // interval exhausted: leave the pool of busy explorers (the
@@ -931,17 +933,19 @@ namespace pbbl {
 
 int smem_bytes(int n, int m, int Ppad, int warps) { return pbb_smem_plan(n, m, Ppad, warps).total; }
 
-int explore_ctas_per_sm(int nw, int warps_per_cta, int smem)
+template <int NW, int SORT>
+int explore_occupancy(int warps_per_cta, int smem)
 {
     int blocks = 0;
-    if (nw == 1) {
-        cudaFuncSetAttribute(pbb_explore_kernel<1>, cudaFuncAttributeMaxDynamicSharedMemorySize, smem);
-        cudaOccupancyMaxActiveBlocksPerMultiprocessor(&blocks, pbb_explore_kernel<1>, 32 * warps_per_cta, smem);
-    } else {
-        cudaFuncSetAttribute(pbb_explore_kernel<2>, cudaFuncAttributeMaxDynamicSharedMemorySize, smem);
-        cudaOccupancyMaxActiveBlocksPerMultiprocessor(&blocks, pbb_explore_kernel<2>, 32 * warps_per_cta, smem);
-    }
+    cudaFuncSetAttribute(pbb_explore_kernel<NW, SORT>, cudaFuncAttributeMaxDynamicSharedMemorySize, smem);
+    cudaOccupancyMaxActiveBlocksPerMultiprocessor(&blocks, pbb_explore_kernel<NW, SORT>, 32 * warps_per_cta, smem);
     return blocks;
+}
+
+int explore_ctas_per_sm(int nw, int warps_per_cta, int smem, int sort)
+{
+    if (nw == 1) return sort ? explore_occupancy<1, 1>(warps_per_cta, smem) : explore_occupancy<1, 0>(warps_per_cta, smem);
+    return sort ? explore_occupancy<2, 1>(warps_per_cta, smem) : explore_occupancy<2, 0>(warps_per_cta, smem);
 }
 
 cudaError_t launch_reset(const DevGroup* groups, int ngroups, const int* ub, cudaStream_t st)
@@ -971,19 +975,28 @@ cudaError_t launch_lower_ub(const DevGroup* groups, int g, int ub, cudaStream_t 
     return cudaGetLastError();
 }
 
-cudaError_t launch_explore(int nw, const DevGroup* groups, const int* ngroups_d, int ctas, int warps_per_cta, int smem,
+template <int NW, int SORT>
+cudaError_t explore_launch(const DevGroup* groups, const int* ngroups_d, int ctas, int warps_per_cta, int smem,
                            unsigned long long budget_ns, int max_rounds, int select_budget, cudaStream_t st)
 {
-    if (nw == 1) {
-        cudaFuncSetAttribute(pbb_explore_kernel<1>, cudaFuncAttributeMaxDynamicSharedMemorySize, smem);
-        pbb_explore_kernel<1><<<ctas, 32 * warps_per_cta, smem, st>>>(groups, ngroups_d, warps_per_cta, budget_ns,
-                                                                       max_rounds, select_budget);
-    } else {
-        cudaFuncSetAttribute(pbb_explore_kernel<2>, cudaFuncAttributeMaxDynamicSharedMemorySize, smem);
-        pbb_explore_kernel<2><<<ctas, 32 * warps_per_cta, smem, st>>>(groups, ngroups_d, warps_per_cta, budget_ns,
-                                                                       max_rounds, select_budget);
-    }
+    cudaFuncSetAttribute(pbb_explore_kernel<NW, SORT>, cudaFuncAttributeMaxDynamicSharedMemorySize, smem);
+    pbb_explore_kernel<NW, SORT><<<ctas, 32 * warps_per_cta, smem, st>>>(groups, ngroups_d, warps_per_cta, budget_ns,
+                                                                          max_rounds, select_budget);
     return cudaGetLastError();
+}
+
+cudaError_t launch_explore(int nw, const DevGroup* groups, const int* ngroups_d, int ctas, int warps_per_cta, int smem,
+                           unsigned long long budget_ns, int max_rounds, int select_budget, cudaStream_t st, int sort)
+{
+    if (nw == 1)
+        return sort ? explore_launch<1, 1>(groups, ngroups_d, ctas, warps_per_cta, smem, budget_ns, max_rounds,
+                                           select_budget, st)
+                    : explore_launch<1, 0>(groups, ngroups_d, ctas, warps_per_cta, smem, budget_ns, max_rounds,
+                                           select_budget, st);
+    return sort ? explore_launch<2, 1>(groups, ngroups_d, ctas, warps_per_cta, smem, budget_ns, max_rounds,
+                                       select_budget, st)
+                : explore_launch<2, 0>(groups, ngroups_d, ctas, warps_per_cta, smem, budget_ns, max_rounds,
+                                       select_budget, st);
 }
 
 cudaError_t launch_bound(int nw, const DevInstance& I, int count, const int* sched, const int* l1, const int* l2,

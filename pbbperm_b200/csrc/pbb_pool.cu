@@ -313,8 +313,8 @@ extern "C" int pbb_pool_submit(pbb_pool* P, const pbb_instance* inst, const pbb_
           c.branching_mode == 2 || c.branching_mode == 3))
         return pfail(PBB_E_INVAL, "adaptiveBranchingMode must be one of -3,-2,-1,1,2,3");
     if (c.early_stop_johnson) return pfail(PBB_E_UNSUPPORTED, "earlyStopJohnson=true is not supported");
-    if (c.sorted_dfs < 0 || c.sorted_dfs > 1)
-        return pfail(PBB_E_UNSUPPORTED, "sortedDFS must be 0 or 1 (2-4 sort by idle-time priorities, not computed here)");
+    if (c.sorted_dfs)
+        return pfail(PBB_E_UNSUPPORTED, "the pool explores with sortedDFS = 0 (the single-instance engine takes 1)");
     const int rc = pbbt::build_tables(inst, c.johnson_mode, r.H);
     if (rc) return rc;
     const int n = inst->n_jobs;
