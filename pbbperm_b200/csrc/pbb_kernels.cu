@@ -686,6 +686,10 @@ pbb_explore_kernel(const DevGroup* groups, const int* ngroups_d, int warps_per_c
     WarpCounters C = {0, 0, 0, 0, 0, 0, 0, 0, 0};
     Ivm<NW> R;
     int cached = -1;                   // explorer whose state is held in registers
+    // explorers holding work once the first PBB_CORE_WARPS warps of every CTA
+    // are busy (no more than that share of the explorers can be)
+    const int core_active = min(PBB_CORE_WARPS * G.ctas,
+                                (int)((long long)G.ivm.count * PBB_CORE_WARPS / warps_per_cta));
     unsigned idle_ns = 500;            // back-off of a warp that found nothing to do
     int best = 0;
     if (lane_id() == 0) best = (int)(ld_volatile_u64(&G.ctl->best_key) >> 32);
@@ -694,9 +698,11 @@ pbb_explore_kernel(const DevGroup* groups, const int* ngroups_d, int warps_per_c
     for (int round = 0; round < max_rounds; round++) {
         // loop control is decided by lane 0 and broadcast, so that the warp
         // never splits on values read at slightly different times
-        int stop = 0;
-        if (lane_id() == 0)
-            stop = ld_volatile_s32(&G.ctl->active) == 0 || globaltimer_ns() - t0 > budget_ns;
+        int stop = 0, active = 0;
+        if (lane_id() == 0) {
+            active = ld_volatile_s32(&G.ctl->active);
+            stop = active == 0 || globaltimer_ns() - t0 > budget_ns;
+        }
         if (__shfl_sync(FULLMASK, stop, 0)) break;
         bool worked = false;
         bool busy = false;          // an explorer of this warp is active or offered
@@ -753,8 +759,13 @@ pbb_explore_kernel(const DevGroup* groups, const int* ngroups_d, int warps_per_c
         }
         // A warp with nothing to do offers ONE of its idle explorers to the
         // donors: work is only split towards warps that would otherwise wait,
-        // never towards a warp that is busy with another explorer.
-        if (!busy && spare >= 0 && lane_id() == 0) {
+        // never towards a warp that is busy with another explorer.  The first
+        // PBB_CORE_WARPS warps of every CTA always take part; the others join
+        // once that many explorers per CTA hold work, so a narrow search is
+        // not cut into pieces for warps it cannot feed, and a wide one still
+        // gets every warp.
+        const bool tier = wic < PBB_CORE_WARPS || active >= core_active;
+        if (!busy && spare >= 0 && lane_id() == 0 && tier) {
             st_release(G.ivm.state + spare, IVM_QUEUED);
             if (!queue_push(G, spare)) st_release(G.ivm.state + spare, IVM_IDLE);
         }

@@ -5,6 +5,9 @@
 #define PBB_MAX_N 64          // jobs per instance (int8 IVM cells, two 32-bit mask words)
 #define PBB_MAX_M 32          // machines per instance (one machine per lane in recurrences)
 #define PBB_WARPS_MAX 20      // explorer warps per CTA (96 registers a thread)
+#ifndef PBB_CORE_WARPS
+#define PBB_CORE_WARPS 8      // warps per CTA that ask for work whatever the search's width
+#endif
 
 // IVM life cycle (per explorer, in global memory)
 #define IVM_IDLE 0            // no interval
