@@ -37,7 +37,7 @@ extern "C" {
 #define PBB_E_INVAL (-1)       /* bad argument or unsupported instance/config */
 #define PBB_E_NOMEM (-2)       /* device allocation failed */
 #define PBB_E_CUDA (-3)        /* CUDA runtime error (message in pbb_last_error) */
-#define PBB_E_TIMEOUT (-4)     /* a device wait ran out of its bound */
+#define PBB_E_TIMEOUT (-4)     /* the host's wait for a window ran out (pbb_set_wait_limit) */
 #define PBB_E_UNSUPPORTED (-5) /* option the engine does not implement */
 
 #define PBB_MAX_JOBS 64
@@ -59,13 +59,19 @@ typedef struct pbb_config {
     int32_t branching_mode;     /* [bb] adaptiveBranchingMode (CPU numbering): -3,-2,-1,1,2,3 */
     int32_t find_all;           /* [bb] findAll */
     int32_t johnson_mode;       /* [bb] JohnsonMode: 0 all pairs, 1 (k,m), 2 (k,k+1) */
-    int32_t early_stop_johnson; /* [bb] earlyStopJohnson: must be 0 */
-    int32_t sorted_dfs;         /* [bb] sortedDFS: 0 (reverse the row on a side change) or 1 (sort it
-                                   by the chosen side's bound, ivm_bound.cpp:344-349); 2-4 rejected */
+    int32_t early_stop_johnson; /* [bb] earlyStopJohnson: 1 = a child's Johnson scan stops once it exceeds
+                                   the incumbent (same nodes; rejected with boundingMode 1 + MaxSum) */
+    int32_t sorted_dfs;         /* [bb] sortedDFS: 0 reverse the row on a side change; 1 sort it by the
+                                   chosen side's bound; 2 and 4 by (bound, priority); 3 by the priority
+                                   (ivm_bound.cpp:338-370) */
     int32_t nb_ivms;            /* [gpu] nbIVMs: explorers */
     int32_t device;             /* CUDA device ordinal */
     int32_t warps_per_cta;      /* 0 = largest that fits shared memory */
     int32_t ctas;               /* 0 = SMs x resident CTAs per SM */
+    int32_t sorting_criterion;  /* [bb] sortingCriterion, the sibling priority of sortedDFS 2-4
+                                   (ivm_bound.cpp:506-544): 1 the chosen side's bound, 2 that bound
+                                   minus the other side's, 3 the weak bound's idle time (not with
+                                   boundingMode 1); 4 is rejected */
 } pbb_config;
 
 typedef struct pbb_stats {
@@ -127,6 +133,13 @@ int pbb_init_from_fac(pbb_engine* e, int32_t ub, const int32_t* root_perm, int32
  * small (the reference exits there); counters are not reset. */
 int pbb_get_intervals(pbb_engine* e, int32_t max_intervals, int32_t* pos, int32_t* end, int32_t* ids,
                       int32_t* nb_intervals);
+
+/* Longest the host waits for one pbb_explore window (seconds): < 0 = the
+ * window's device time + 60 s (default), 0 = no limit.  When the wait runs
+ * out, pbb_explore returns PBB_E_TIMEOUT; the window still ends by its own
+ * device-time budget, and the next call on the engine waits for it and
+ * accounts for its work, so counters and intervals stay consistent. */
+int pbb_set_wait_limit(pbb_engine* e, double seconds);
 
 /* Lower the incumbent to `ub` (a bound found by another solver; no
  * permutation is attached): solution::updateCost (common/src/solution.cpp:44-56). */
@@ -211,7 +224,8 @@ int pbb_bound_children(const pbb_instance* inst, int32_t johnson_mode, int32_t d
  * cudaGetSymbolAddress -- make it before any stream capture.  Calls share the
  * array: calls that overlap on the GPU race, so do not issue them
  * concurrently (the function serialises its own host callers and waits for
- * `stream` before returning).  Outputs as pbb_bound_children; all required. */
+ * `stream` before returning).  The calling thread's current device is left as
+ * it was.  Outputs as pbb_bound_children; all required. */
 int pbb_bound_children_noalloc(const pbb_instance* inst, int32_t johnson_mode, int32_t device, void* stream,
                                int32_t count, const int32_t* sched, const int32_t* limit1, const int32_t* limit2,
                                int32_t* weak_begin, int32_t* weak_end, int32_t* strong_begin, int32_t* strong_end,

@@ -21,7 +21,8 @@ int pbb_diag_int32_peak(int32_t device, double* gops, double* seconds);
  * and the direct per-child scans (children, free jobs summed over them). */
 typedef struct pbb_work {
     double device_seconds;
-    int32_t n_jobs, n_machines, machine_pairs, explorers, warps, pad;
+    int32_t n_jobs, n_machines, machine_pairs, explorers, warps;
+    int32_t status;                               /* PBB_ST_* bits the kernels raised */
     uint64_t decomposed, simple_bounds, johnson_bounds;
     uint64_t johnson_sweeps, sweep_free_jobs, sweep_children;
     uint64_t direct_children, direct_free_jobs;   /* children bounded by direct scans */
@@ -42,6 +43,32 @@ int pbb_diag_bound_children(const struct pbb_instance* inst, int32_t johnson_mod
 
 struct pbb_engine;
 int pbb_work_counters(struct pbb_engine* e, pbb_work* out);
+
+/* Status bit of pbb_work.status: 1 = a node the bound kernel rejected. */
+#define PBB_DIAG_ST_BADINPUT 1
+
+/* Limits of the explorer loop for tests of the bounded waits: at most
+ * `select_budget` selection steps per explorer step (then the explorer
+ * yields with its state consistent) and `max_rounds` loop rounds per window
+ * launch (the window then ends early).  Defaults: 4096 and unbounded. */
+int pbb_diag_set_step_limits(struct pbb_engine* e, int32_t select_budget, int32_t max_rounds);
+
+/* Node sampling, for LB parity of the explorer's own bound code: from the
+ * next pbb_explore on, the explorer records nodes it bounds -- those whose
+ * hash of (explorer id, the warp's decomposed count) has its low `rate_log2`
+ * bits clear -- until `capacity` records are taken (recording never waits).
+ * capacity 0 turns sampling off.  A record is 8 + 5 n ints:
+ *   [0] explorer id, [1] line (depth), [2] limit1, [3] limit2,
+ *   [4] side chosen (0 front, 1 back), [5] incumbent when bounded,
+ *   [6] free jobs, [7] 0,
+ *   then n ints of schedule (front jobs, free jobs, back jobs: the
+ *   reference's node->schedule), then n each of weak LB front, weak LB back,
+ *   Johnson LB front, Johnson LB back, by job id, exactly as the explorer
+ *   computed them before pruning (0 = not evaluated). */
+int pbb_diag_sample_nodes(struct pbb_engine* e, int32_t capacity, int32_t rate_log2);
+/* Copy up to max_records records; *count = records copied (max_records <= 0:
+ * records available). */
+int pbb_diag_get_samples(struct pbb_engine* e, int32_t max_records, int32_t* out, int32_t* count);
 
 #ifdef __cplusplus
 }

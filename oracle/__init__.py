@@ -34,7 +34,8 @@ def build_oracle(force=False):
 
 class _OrcCfg(ctypes.Structure):
     _fields_ = [("bound_mode", ctypes.c_int), ("branch_mode", ctypes.c_int),
-                ("find_all", ctypes.c_int), ("sort_nodes", ctypes.c_int), ("node_limit", ctypes.c_int64)]
+                ("find_all", ctypes.c_int), ("sort_nodes", ctypes.c_int), ("node_limit", ctypes.c_int64),
+                ("sort_crit", ctypes.c_int)]
 
 
 class _OrcResult(ctypes.Structure):
@@ -158,8 +159,9 @@ class Oracle:
         return c, perm
 
     def solve(self, ub, bound_mode=2, branch_mode=3, find_all=False, root=None, node_limit=0, pos=None, end=None,
-              sorted_dfs=0):
-        cfg = _OrcCfg(bound_mode, branch_mode, 1 if find_all else 0, int(sorted_dfs), node_limit)
+              sorted_dfs=0, sorting_criterion=1):
+        cfg = _OrcCfg(bound_mode, branch_mode, 1 if find_all else 0, int(sorted_dfs), node_limit,
+                      int(sorting_criterion))
         res = _OrcResult()
         root = np.arange(self.n, dtype=np.int32) if root is None else np.ascontiguousarray(root, dtype=np.int32)
         perm = np.zeros(self.n, np.int32)
@@ -198,6 +200,8 @@ class Reference:
             L.ref_weak_children.argtypes = [_i32p, ctypes.c_int, ctypes.c_int, _i32p, _i32p, _i32p, _i32p]
             L.ref_strong_node.argtypes = [_i32p, ctypes.c_int, ctypes.c_int]
             L.ref_johnson_row.argtypes = [ctypes.c_int, _i32p]
+            L.ref_children_batch.argtypes = [ctypes.c_int, ctypes.c_int, _i32p, _i32p, _i32p, _i32p, _i32p,
+                                             _i32p, _i32p, _i32p, _i32p]
             Reference._L = L
         p = np.ascontiguousarray(p, dtype=np.int32)
         self.m, self.n = p.shape
@@ -234,6 +238,21 @@ class Reference:
         Reference._L.ref_johnson_row(s, _ptr(out))
         return out
 
+    def children_batch(self, sched, l1, l2, want_front, want_back):
+        """Reference children LBs of many nodes: weak front/back of every free
+        job, Johnson of the children flagged in want_front / want_back (all
+        (count, n) arrays by job id; 0 where not computed)."""
+        sched = np.ascontiguousarray(sched, dtype=np.int32)
+        cnt, n = sched.shape
+        l1 = np.ascontiguousarray(l1, dtype=np.int32)
+        l2 = np.ascontiguousarray(l2, dtype=np.int32)
+        wf = np.ascontiguousarray(want_front, dtype=np.int32)
+        wk = np.ascontiguousarray(want_back, dtype=np.int32)
+        out = [np.zeros((cnt, n), np.int32) for _ in range(4)]
+        Reference._L.ref_children_batch(cnt, n, _ptr(sched), _ptr(l1), _ptr(l2), _ptr(wf), _ptr(wk),
+                                        *[_ptr(o) for o in out])
+        return out
+
 
 def write_vrf(dirpath, name, p, ub=None):
     """Write `p` (m x n) as a VRF instance the reference can read
@@ -251,10 +270,13 @@ def write_vrf(dirpath, name, p, ub=None):
 
 
 def run_reference_bb(p, ub=None, bound_mode=2, branch_mode=3, threads=0, johnson=True,
-                     time_limit=None, find_all=False, timeout=3600, sorted_dfs=0):
+                     time_limit=None, find_all=False, timeout=3600, sorted_dfs=0, early_stop=False,
+                     johnson_mode=0, sorting_criterion=-1):
     """Run the reference multicore B&B (oracle/_ref/bb or bbJ) on instance p.
 
-    ub=None means UB=+inf.  Returns the parsed stats dict."""
+    ub=None means UB=+inf.  The ini keys follow common/src/arguments.cpp:80-132
+    (earlyStopJohnson, JohnsonMode, sortedDFS, sortingCriterion).  Returns the
+    parsed stats dict."""
     exe = os.path.join(REF_DIR, "bbJ" if johnson else "bb")
     with tempfile.TemporaryDirectory(prefix="pbbrun_") as d:
         name = "VPBB%dx%d" % (p.shape[1], p.shape[0])
@@ -262,9 +284,12 @@ def run_reference_bb(p, ub=None, bound_mode=2, branch_mode=3, threads=0, johnson
         with open(os.path.join(d, "mcconfig.ini"), "w") as f:
             f.write("[problem]\nproblem = flowshop\ninstance = %s\n" % name)
             f.write("[initial]\nub = %d\n" % (0 if ub is not None else 3))
-            f.write("[bb]\nsingleNode = true\nsortedDFS = %d\nsortingCriterion = -1\n" % sorted_dfs)
-            f.write("boundingMode = %d\nadaptiveBranchingMode = %d\nJohnsonMode = 0\n" % (bound_mode, branch_mode))
-            f.write("earlyStopJohnson = false\nfindAll = %s\n" % ("true" if find_all else "false"))
+            f.write("[bb]\nsingleNode = true\nsortedDFS = %d\nsortingCriterion = %d\n"
+                    % (sorted_dfs, sorting_criterion))
+            f.write("boundingMode = %d\nadaptiveBranchingMode = %d\nJohnsonMode = %d\n"
+                    % (bound_mode, branch_mode, johnson_mode))
+            f.write("earlyStopJohnson = %s\nfindAll = %s\n" % ("true" if early_stop else "false",
+                                                              "true" if find_all else "false"))
             f.write("[verbose]\nprintSolutions = false\n")
             f.write("[multicore]\nthreads = %d\nworksteal = o\n" % threads)
         env = dict(os.environ)

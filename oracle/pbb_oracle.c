@@ -370,8 +370,11 @@ typedef struct {
     int bound_mode;    /* [bb] boundingMode: 0 weak, 1 strong, 2 weak then strong */
     int branch_mode;   /* [bb] adaptiveBranchingMode: -3,-2,-1,1,2,3 (CPU numbering) */
     int find_all;      /* [bb] findAll */
-    int sort_nodes;    /* [bb] sortedDFS: 0 (row reversal) or 1 (rows sorted by the first cost) */
+    int sort_nodes;    /* [bb] sortedDFS: 0 row reversal; 1 sort by the first cost; 2, 4 by (first
+                          cost, priority); 3 by priority (ivm_bound.cpp:338-370) */
     int64_t node_limit;/* stop after this many decomposed nodes (<=0: none) */
+    int sort_crit;     /* [bb] sortingCriterion: priority of siblings, 1 chosen side's cost,
+                          2 its difference with the other side's, 3 idle time (:506-544) */
 } orc_cfg;
 
 typedef struct {
@@ -394,6 +397,8 @@ typedef struct {
     int *best_perm;
     /* per-node cost tables indexed by job (ivm_bound.cpp:27-31) */
     int cb_w[ORC_MAXN], ce_w[ORC_MAXN], cb_s[ORC_MAXN], ce_s[ORC_MAXN];
+    int pb_w[ORC_MAXN], pe_w[ORC_MAXN];   /* weak idle-time priorities (priorityBegin/End) */
+    int prio[ORC_MAXN];                   /* sibling priorities set by chooseChildrenSet */
     orc_result res;
 } orc_bb;
 
@@ -439,11 +444,10 @@ static void prepare_schedule(orc_bb *B)
 
 static void weak_bounds(orc_bb *B)                              /* ivm_bound.cpp:216-236 */
 {
-    int pb[ORC_MAXN], pe[ORC_MAXN];
     memset(B->cb_s, 0, sizeof(int) * B->n);
     memset(B->ce_s, 0, sizeof(int) * B->n);
     int both = B->cfg.branch_mode > 0;
-    orc_weak_children(B->I, B->sched, B->l1, B->l2, both, B->cb_w, B->ce_w, pb, pe);
+    orc_weak_children(B->I, B->sched, B->l1, B->l2, both, B->cb_w, B->ce_w, B->pb_w, B->pe_w);
     B->res.simple_bounds += both ? 2 * (B->l2 - B->l1 - 1) : (B->l2 - B->l1 - 1);
 }
 
@@ -467,8 +471,10 @@ static void strong_bounds(orc_bb *B, int front_side)
     }
 }
 
-/* ivm_bound.cpp:413-560 (CPU rule numbering); 0 = FRONT, 1 = BACK */
-static int choose_dir(const orc_bb *B, const int *cb, const int *ce)
+/* ivm_bound.cpp:413-504 (CPU rule numbering); 0 = FRONT, 1 = BACK.  The
+ * multicore B&B forces singleNode (multicore/src/main.cpp:21), so MinBranch
+ * and MinMin count pruned children against the incumbent (:458-459). */
+static int choose_side(const orc_bb *B, const int *cb, const int *ce)
 {
     int n = B->n, ub = B->best;
     switch (B->cfg.branch_mode) {
@@ -510,6 +516,23 @@ static int choose_dir(const orc_bb *B, const int *cb, const int *ce)
     }
 }
 
+/* chooseChildrenSet (ivm_bound.cpp:413-560): the side, then the siblings'
+ * priorities for sortedDFS 2-4 (:506-544).  Priority 3 reads the weak
+ * bound's idle times (priorityBegin/End); criteria 4 and the strong bound's
+ * idle times are rejected by the engine and never reach here. */
+static int choose_dir(orc_bb *B, const int *cb, const int *ce)
+{
+    int n = B->n;
+    int side = choose_side(B, cb, ce);
+    for (int i = 0; i < n; i++) {
+        int mine = side ? ce[i] : cb[i], other = side ? cb[i] : ce[i];
+        if (B->cfg.sort_crit == 1) B->prio[i] = mine;
+        else if (B->cfg.sort_crit == 2) B->prio[i] = mine - other;
+        else if (B->cfg.sort_crit == 3) B->prio[i] = mine > 0 ? (side ? B->pe_w[i] : B->pb_w[i]) : 99999;
+    }
+    return side;
+}
+
 /* misc.h:33-48 gnomeSortByKeyInc: stable, swaps neighbours while the left key
  * is strictly larger */
 static void gnome_sort_by_key(int *arr, const int *key, int from, int to)
@@ -524,9 +547,24 @@ static void gnome_sort_by_key(int *arr, const int *key, int from, int to)
     }
 }
 
+/* misc.h:50-65 gnomeSortByKeysInc: the same, with key2 breaking ties of key1 */
+static void gnome_sort_by_keys(int *arr, const int *key1, const int *key2, int from, int to)
+{
+    int i = from + 1, j = i + 1;
+    while (i <= to) {
+        if (key1[arr[i - 1]] > key1[arr[i]] ||
+            (key1[arr[i - 1]] == key1[arr[i]] && key2[arr[i - 1]] > key2[arr[i]])) {
+            int t = arr[i - 1]; arr[i - 1] = arr[i]; arr[i] = t;
+            if (--i) continue;
+        }
+        i = j++;
+    }
+}
+
 /* ivm_bound.cpp:611-646 -> eliminateJobs :338-410.  sortedDFS = 0 reverses the
  * row when the side changes; sortedDFS = 1 sorts it by the chosen side's first
- * cost instead (:344-349). */
+ * cost instead (:344-349), 2 and 4 by that cost then the priority (:350-354,
+ * :360-364), 3 by the priority (:355-359). */
 static void prune(orc_bb *B, const int *c1b, const int *c1e, const int *c2b, const int *c2e)
 {
     int n = B->n, l = B->line;
@@ -538,6 +576,8 @@ static void prune(orc_bb *B, const int *c1b, const int *c1e, const int *c2b, con
     const int *c1 = B->dir[l] == 1 ? c1e : c1b;
     const int *c2 = B->dir[l] == 1 ? c2e : c2b;
     if (B->cfg.sort_nodes == 1) gnome_sort_by_key(row, c1, 0, n - l - 1);
+    else if (B->cfg.sort_nodes == 2 || B->cfg.sort_nodes == 4) gnome_sort_by_keys(row, c1, B->prio, 0, n - l - 1);
+    else if (B->cfg.sort_nodes == 3) gnome_sort_by_key(row, B->prio, 0, n - l - 1);
     for (int i = 0; i < n - l; i++) {
         int j = row[i];
         if (gt_best(B, c1[j]) || gt_best(B, c2[j])) row[i] = flag_neg(j);

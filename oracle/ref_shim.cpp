@@ -91,4 +91,38 @@ void ref_johnson_row(int s, int* out) {
     memcpy(out, bound_fsp_strong::tabJohnson + s * g_n, g_n * sizeof(int));
 }
 
+// Reference children bounds of `count` nodes (schedule row-major count x n,
+// node i fixes sched[0..l1[i]] in front and sched[l2[i]..n) at the back):
+// weak front / back LBs of every free job (boundChildren), and the Johnson LB
+// of each child whose entry in want_front / want_back is nonzero, computed as
+// ivm_bound::computeStrongBounds does (multicore/src/ivm_bound.cpp:141-195):
+// the child's job swapped into the fill slot, bornes_calculer with no early
+// exit.  All outputs by job id, 0 where not computed.
+void ref_children_batch(int count, int n, const int* sched, const int* l1, const int* l2, const int* want_front,
+                        const int* want_back, int* wb, int* we, int* sb, int* se) {
+    int s[1024], pb[1024], pe[1024];
+    for (int i = 0; i < count; i++) {
+        const int* sc = sched + (size_t)i * n;
+        const int a = l1[i], b = l2[i];
+        memcpy(s, sc, n * sizeof(int));
+        g_weak->boundChildren(s, a, b, wb + (size_t)i * n, we + (size_t)i * n, pb, pe);
+        for (int j = 0; j < n; j++) { sb[(size_t)i * n + j] = 0; se[(size_t)i * n + j] = 0; }
+        for (int side = 0; side < 2; side++) {
+            const int* want = (side == 0 ? want_front : want_back) + (size_t)i * n;
+            int* out = (side == 0 ? sb : se) + (size_t)i * n;
+            const int L1 = a + (side == 0 ? 1 : 0), L2 = b - (side == 0 ? 0 : 1);
+            const int fill = side == 0 ? L1 : L2;
+            for (int q = a + 1; q < b; q++) {
+                const int job = sc[q];
+                if (!want[job]) continue;
+                memcpy(s, sc, n * sizeof(int));
+                const int t = s[fill]; s[fill] = s[q]; s[q] = t;
+                int c[2] = {0, 0};
+                g_strong->bornes_calculer(s, L1, L2, c, -1);
+                out[job] = c[0];
+            }
+        }
+    }
+}
+
 }

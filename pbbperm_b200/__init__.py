@@ -49,7 +49,8 @@ class _Config(ctypes.Structure):
                 ("find_all", ctypes.c_int32), ("johnson_mode", ctypes.c_int32),
                 ("early_stop_johnson", ctypes.c_int32), ("sorted_dfs", ctypes.c_int32),
                 ("nb_ivms", ctypes.c_int32), ("device", ctypes.c_int32),
-                ("warps_per_cta", ctypes.c_int32), ("ctas", ctypes.c_int32)]
+                ("warps_per_cta", ctypes.c_int32), ("ctas", ctypes.c_int32),
+                ("sorting_criterion", ctypes.c_int32)]
 
 
 class _Stats(ctypes.Structure):
@@ -67,7 +68,7 @@ class _Result(ctypes.Structure):
 class _Work(ctypes.Structure):
     _fields_ = [("device_seconds", ctypes.c_double), ("n_jobs", ctypes.c_int32), ("n_machines", ctypes.c_int32),
                 ("machine_pairs", ctypes.c_int32), ("explorers", ctypes.c_int32), ("warps", ctypes.c_int32),
-                ("pad", ctypes.c_int32), ("decomposed", ctypes.c_uint64), ("simple_bounds", ctypes.c_uint64),
+                ("status", ctypes.c_int32), ("decomposed", ctypes.c_uint64), ("simple_bounds", ctypes.c_uint64),
                 ("johnson_bounds", ctypes.c_uint64), ("johnson_sweeps", ctypes.c_uint64),
                 ("sweep_free_jobs", ctypes.c_uint64), ("sweep_children", ctypes.c_uint64),
                 ("direct_children", ctypes.c_uint64), ("direct_free_jobs", ctypes.c_uint64)]
@@ -112,6 +113,10 @@ def lib():
         L.pbb_get_intervals.argtypes = [ctypes.c_void_p, ctypes.c_int32, _i32p, _i32p, _i32p,
                                         ctypes.POINTER(ctypes.c_int32)]
         L.pbb_set_ub.argtypes = [ctypes.c_void_p, ctypes.c_int32]
+        L.pbb_set_wait_limit.argtypes = [ctypes.c_void_p, ctypes.c_double]
+        L.pbb_diag_set_step_limits.argtypes = [ctypes.c_void_p, ctypes.c_int32, ctypes.c_int32]
+        L.pbb_diag_sample_nodes.argtypes = [ctypes.c_void_p, ctypes.c_int32, ctypes.c_int32]
+        L.pbb_diag_get_samples.argtypes = [ctypes.c_void_p, ctypes.c_int32, _i32p, ctypes.POINTER(ctypes.c_int32)]
         L.pbb_work_counters.argtypes = [ctypes.c_void_p, ctypes.POINTER(_Work)]
         L.pbb_diag_bound_children.argtypes = [ctypes.POINTER(_Instance), ctypes.c_int32, ctypes.c_int32,
                                                ctypes.c_int32, ctypes.c_int32, _i32p, _i32p, _i32p, _i32p, _i32p,
@@ -153,7 +158,8 @@ class Config:
     """Search settings, named after the reference ini keys."""
 
     def __init__(self, boundingMode=2, adaptiveBranchingMode=3, findAll=False, JohnsonMode=0,
-                 earlyStopJohnson=False, sortedDFS=0, nbIVMs=16384, device=0, warps_per_cta=0, ctas=0):
+                 earlyStopJohnson=False, sortedDFS=0, nbIVMs=16384, device=0, warps_per_cta=0, ctas=0,
+                 sortingCriterion=1):
         self.boundingMode = boundingMode
         self.adaptiveBranchingMode = adaptiveBranchingMode
         self.findAll = findAll
@@ -164,11 +170,12 @@ class Config:
         self.device = device
         self.warps_per_cta = warps_per_cta
         self.ctas = ctas
+        self.sortingCriterion = sortingCriterion
 
     def _c(self):
         return _Config(self.boundingMode, self.adaptiveBranchingMode, 1 if self.findAll else 0, self.JohnsonMode,
                        1 if self.earlyStopJohnson else 0, self.sortedDFS, self.nbIVMs, self.device,
-                       self.warps_per_cta, self.ctas)
+                       self.warps_per_cta, self.ctas, self.sortingCriterion)
 
 
 def _result(r):
@@ -255,6 +262,44 @@ class Engine:
         """Lower the incumbent to a bound found elsewhere (no permutation)."""
         _check(lib().pbb_set_ub(self._h, int(ub)))
 
+    def set_wait_limit(self, seconds):
+        """Longest host wait for one window (< 0: window + 60 s, 0: none);
+        explore() raises PbbError(PBB_E_TIMEOUT) when it runs out, and the
+        next call accounts for the window."""
+        _check(lib().pbb_set_wait_limit(self._h, float(seconds)))
+
+    def sample_nodes(self, capacity, rate_log2):
+        """Diagnostic: from the next window on, record nodes the explorer
+        bounds (hash-sampled at 2^-rate_log2, at most `capacity`; 0 = off)."""
+        _check(lib().pbb_diag_sample_nodes(self._h, int(capacity), int(rate_log2)))
+
+    def sample_count(self):
+        """Nodes recorded so far (at most the capacity)."""
+        cnt = ctypes.c_int32(0)
+        _check(lib().pbb_diag_get_samples(self._h, 0, None, ctypes.byref(cnt)))
+        return cnt.value
+
+    def samples(self):
+        """Recorded nodes as a dict of arrays: explorer, line, limit1, limit2,
+        side, best, k (count,) and sched, weak_begin, weak_end, strong_begin,
+        strong_end (count, n) -- include/pbbperm_diag.h's record layout."""
+        n = self.n
+        cnt = ctypes.c_int32(0)
+        _check(lib().pbb_diag_get_samples(self._h, 0, None, ctypes.byref(cnt)))
+        stride = 8 + 5 * n
+        buf = np.zeros((max(1, cnt.value), stride), np.int32)
+        _check(lib().pbb_diag_get_samples(self._h, cnt.value, _ptr(buf), ctypes.byref(cnt)))
+        buf = buf[:cnt.value]
+        out = {k: buf[:, i].copy() for i, k in enumerate(("explorer", "line", "limit1", "limit2", "side", "best", "k"))}
+        for i, k in enumerate(("sched", "weak_begin", "weak_end", "strong_begin", "strong_end")):
+            out[k] = buf[:, 8 + i * n: 8 + (i + 1) * n].copy()
+        return out
+
+    def set_step_limits(self, select_budget=4096, max_rounds=2**31 - 1):
+        """Diagnostic: selection steps per explorer step and loop rounds per
+        window launch (tests of the bounded loops)."""
+        _check(lib().pbb_diag_set_step_limits(self._h, int(select_budget), int(max_rounds)))
+
     def kernel_stats(self):
         """Work of the explorer kernels since start, with the INT32 op model
         of the bounds: weak child 5m ops (add/max chain per machine); per
@@ -272,7 +317,7 @@ class Engine:
                     johnson_sweeps=w.johnson_sweeps, sweep_free_jobs=w.sweep_free_jobs,
                     sweep_children=w.sweep_children, direct_children=w.direct_children,
                     direct_free_jobs=w.direct_free_jobs,
-                    explorers=w.explorers, warps=w.warps,
+                    explorers=w.explorers, warps=w.warps, status=w.status,
                     work_model="5m per weak child + P*(10 per swept free job + 9 per swept child)"
                                " + P*4 per free job of a directly scanned child")
 

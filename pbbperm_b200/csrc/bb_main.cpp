@@ -35,7 +35,7 @@ namespace {
 struct Args {
     std::string problem = "flowshop", inst = "UNKNOWN", inifile = "./gpuconfig.ini";
     int init_mode = -1, init_sol = 0;
-    int bound_mode = 2, branch_mode = 3, johnson_mode = 1, sorted = 1, nb_ivms = 4096;
+    int bound_mode = 2, branch_mode = 3, johnson_mode = 1, sorted = 1, sort_crit = 1, nb_ivms = 4096;
     bool early_stop = true, find_all = false, print_solutions = false;
     double time_limit = 0;
 };
@@ -173,6 +173,7 @@ int main(int argc, char** argv)
         a.init_sol = (int)ini.get_int("initial", "sol", 0);
         a.nb_ivms = (int)ini.get_int("gpu", "nbIVMs", 4096);
         a.sorted = (int)ini.get_int("bb", "sortedDFS", 1);
+        a.sort_crit = (int)ini.get_int("bb", "sortingCriterion", 1);
         a.early_stop = ini.get_bool("bb", "earlyStopJohnson", true);
         a.bound_mode = (int)ini.get_int("bb", "boundingMode", 2);
         a.johnson_mode = (int)ini.get_int("bb", "JohnsonMode", 1);
@@ -231,6 +232,7 @@ int main(int argc, char** argv)
     cfg.johnson_mode = a.johnson_mode;
     cfg.early_stop_johnson = a.early_stop;
     cfg.sorted_dfs = a.sorted;
+    cfg.sorting_criterion = a.sort_crit;
     cfg.nb_ivms = a.nb_ivms;
     pbb_engine* e = nullptr;
     struct timespec ts, te;

@@ -10,6 +10,7 @@
 #pragma once
 #include <cuda_runtime.h>
 #include <stdint.h>
+#include <climits>
 #include "pbb_types.h"
 
 #define FULLMASK 0xffffffffu
@@ -315,6 +316,35 @@ __device__ __forceinline__ int weak_back(const CtaTables& T, const WarpScratch& 
     return lb;
 }
 
+// idle-time priority of child u appended at the front: the sum over machines
+// k >= 1 of |completion of u on k-1 - front_k| (bound_fsp_weak.cpp:140-146)
+__device__ __forceinline__ int weak_front_idle(const CtaTables& T, const WarpScratch& S, int u)
+{
+    const int n = T.n;
+    int t0 = S.Fb[0] + T.p[u];
+    int pr = 0;
+    PBB_ROLLED
+    for (int k = 1; k < T.m; k++) {
+        pr += abs(t0 - S.Fb[k]);
+        t0 = max(S.Fb[k], t0) + T.p[k * n + u];
+    }
+    return pr;
+}
+
+// the same for child u prepended at the back (bound_fsp_weak.cpp:172-178)
+__device__ __forceinline__ int weak_back_idle(const CtaTables& T, const WarpScratch& S, int u)
+{
+    const int n = T.n, m = T.m;
+    int t0 = S.Bb[m - 1] + T.p[(m - 1) * n + u];
+    int pr = 0;
+    PBB_ROLLED
+    for (int k = m - 2; k >= 0; k--) {
+        pr += abs(t0 - S.Bb[k]);
+        t0 = max(t0, S.Bb[k]) + T.p[k * n + u];
+    }
+    return pr;
+}
+
 // makespan of  front jobs + x + y + back jobs  (y < 0: front + x + back),
 // as max over machines of head + tail at the split
 __device__ __forceinline__ int makespan_split(const CtaTables& T, const WarpScratch& S, int x, int y)
@@ -552,10 +582,14 @@ __device__ __forceinline__ void direct_start(const CtaTables& T, const WarpScrat
 // that the loop body has no branch (cutting the walk at the own positions
 // instead made the lanes of a warp diverge and ran slower).  Chains past the
 // child count repeat the first child and are not stored.  Child maxima over
-// the pairs are taken with one warp reduction per pass.
+// the pairs are taken with one warp reduction per pass.  Early exit
+// (earlyStopJohnson, bound_fsp_strong.cpp:154-158): once every child's
+// running maximum exceeds `stop` the remaining passes are skipped; such a
+// child is pruned whatever its remaining pairs give, so only the value of a
+// pruned child changes (INT_MAX = no early exit).
 template <int C, int NW>
 __device__ __forceinline__ void johnson_direct_chains(const CtaTables& T, const WarpScratch& S, int k, int nc,
-                                                      const int (&cjob)[4], const int (&cside)[4])
+                                                      const int (&cjob)[4], const int (&cside)[4], int stop)
 {
     typedef typename PosMask<NW>::type M;
     const int lane = lane_id();
@@ -597,8 +631,13 @@ __device__ __forceinline__ void johnson_direct_chains(const CtaTables& T, const 
 #pragma unroll
             for (int c = 0; c < C; c++) v[c] = max(t1[c] + B1[c], t0[c] + B0[c]);
         }
+        bool over = true;
 #pragma unroll
-        for (int c = 0; c < C; c++) acc[c] = max(acc[c], __reduce_max_sync(FULLMASK, v[c]));
+        for (int c = 0; c < C; c++) {
+            acc[c] = max(acc[c], __reduce_max_sync(FULLMASK, v[c]));
+            over = over && acc[c] > stop;
+        }
+        if (over) break;
     }
     if (lane == 0) {
 #pragma unroll
@@ -614,12 +653,12 @@ __device__ __forceinline__ void johnson_direct_chains(const CtaTables& T, const 
 
 template <int NW>
 __device__ __forceinline__ void johnson_direct_masked(const CtaTables& T, const WarpScratch& S, int k, int nc,
-                                                      const int (&cjob)[4], const int (&cside)[4])
+                                                      const int (&cjob)[4], const int (&cside)[4], int stop)
 {
     static_assert(PBB_DIRECT_MAX <= 4, "direct scans walk at most four children together");
     if (nc <= 0) return;
-    if (nc <= 2) johnson_direct_chains<2, NW>(T, S, k, nc, cjob, cside);
-    else johnson_direct_chains<4, NW>(T, S, k, nc, cjob, cside);
+    if (nc <= 2) johnson_direct_chains<2, NW>(T, S, k, nc, cjob, cside, stop);
+    else johnson_direct_chains<4, NW>(T, S, k, nc, cjob, cside, stop);
 }
 
 // johnson_children (forward + backward max-plus sweeps) over the free
@@ -819,15 +858,17 @@ struct NodeCounters {
 // :650-676 -> chooseChildrenSet, prune :611-646 with sortedDFS = 0).
 // Stable sort of a row's k cells (k <= 64; lane l holds cells l and 32 + l) by
 // key, written to out[0..k): a cell's place = cells with a smaller key plus
-// earlier cells with the same key, the order gnomeSortByKeyInc (misc.h:33-48)
-// leaves.  Called by all 32 lanes.
-__device__ __noinline__ void sort_cells(unsigned char* out, int k, int key0, int key1, int cell0, int cell1)
+// earlier cells with the same key, the order gnomeSortByKeyInc and
+// gnomeSortByKeysInc (misc.h:33-65) leave.  Keys are 64-bit so that a
+// (cost, priority) pair sorts as one.  Called by all 32 lanes.
+__device__ __noinline__ void sort_cells(unsigned char* out, int k, unsigned long long key0, unsigned long long key1,
+                                        int cell0, int cell1)
 {
     const int lane = lane_id();
     int r0 = 0, r1 = 0;
     PBB_ROLLED
     for (int j = 0; j < k; j++) {
-        const int kj = __shfl_sync(FULLMASK, j < 32 ? key0 : key1, j & 31);
+        const unsigned long long kj = __shfl_sync(FULLMASK, j < 32 ? key0 : key1, j & 31);
         r0 += (kj < key0 || (kj == key0 && j < lane)) ? 1 : 0;
         r1 += (kj < key1 || (kj == key1 && j < lane + 32)) ? 1 : 0;
     }
@@ -836,11 +877,14 @@ __device__ __noinline__ void sort_cells(unsigned char* out, int k, int key0, int
     __syncwarp();
 }
 
-// Returns the side chosen for this level.
-template <int NW, int SORT = 1>
+// Returns the side chosen for this level.  SAMPLE = 1 with `rec` set writes
+// the children's bounds, as computed and before pruning, into a node record
+// (SampleBuf layout: schedule at rec + PBB_SAMPLE_HDR, then four arrays of n).
+template <int NW, int SORT = 1, int SAMPLE = 0>
 __device__ __forceinline__ int bound_and_prune(const CtaTables& T, const WarpScratch& S, const DevSearch& srch,
                                                int mode, int (&row)[NW], int k, int f, int b, int line,
-                                               int prev_dir, int best, NodeCounters& cnt, bool partial_ready = false)
+                                               int prev_dir, int best, NodeCounters& cnt, bool partial_ready = false,
+                                               int* rec = nullptr)
 {
     const int lane = lane_id();
     bool valid[NW];
@@ -931,7 +975,10 @@ __device__ __forceinline__ int bound_and_prune(const CtaTables& T, const WarpScr
                             }
                         }
                     }
-                    if (T.posj) johnson_direct_masked<NW>(T, S, k, nc, cjob, cside);
+                    // the early exit lives in the runtime-options build only (SORT = 1):
+                    // the default explorer passes a constant and keeps no trace of it
+                    const int stop = (SORT && srch.early_stop) ? best : INT_MAX;
+                    if (T.posj) johnson_direct_masked<NW>(T, S, k, nc, cjob, cside, stop);
                     else johnson_direct<NW>(T, S, um, nc, cjob, cside);
                     cnt.direct_children += nc;
                     cnt.direct_free += (unsigned long long)nc * k;
@@ -952,6 +999,24 @@ __device__ __forceinline__ int bound_and_prune(const CtaTables& T, const WarpScr
         if (mode == 1) dir = choose_dir<NW>(srch.branch_mode, line, best, cbs, ces, valid);
     }
 
+    if (SAMPLE && rec) {
+        const int n = T.n;
+        int* sch = rec + PBB_SAMPLE_HDR;
+#pragma unroll
+        for (int w = 0; w < NW; w++) {
+            if (valid[w]) {
+                const int u = row[w];
+                sch[f + w * 32 + lane] = u;
+                sch[n + u] = cbw[w];
+                sch[2 * n + u] = cew[w];
+                sch[3 * n + u] = cbs[w];
+                sch[4 * n + u] = ces[w];
+            }
+        }
+        if (lane == 0) rec[4] = dir;
+        __syncwarp();
+    }
+
     // prune: mark children whose bound reaches the incumbent (eliminateJobs :338-410)
 #pragma unroll
     for (int w = 0; w < NW; w++) {
@@ -963,12 +1028,32 @@ __device__ __forceinline__ int bound_and_prune(const CtaTables& T, const WarpScr
         if (valid[w] && cut) row[w] = cell_flag(row[w]);
     }
     if (SORT && srch.sort_nodes) {
-        // sortedDFS = 1: eliminateJobs sorts the row by the chosen side's first
-        // cost (ivm_bound.cpp:344-349), out of line to keep the hot loop small
-        int key[NW];
+        // sortedDFS >= 1: eliminateJobs sorts the row (ivm_bound.cpp:338-370)
+        // by the chosen side's first cost, then (2, 4) by the sibling
+        // priority chooseChildrenSet set (:506-544), or (3) by the priority
+        // alone; out of line to keep the hot loop small.  The first cost is
+        // also the cost the side was chosen from (weak, or Johnson in mode 1).
+        unsigned long long key[NW];
 #pragma unroll
-        for (int w = 0; w < NW; w++) key[w] = (mode == 1) ? (dir ? ces[w] : cbs[w]) : (dir ? cew[w] : cbw[w]);
-        sort_cells(S.rowj, k, key[0], NW > 1 ? key[NW - 1] : 0, row[0], NW > 1 ? row[NW - 1] : 0);
+        for (int w = 0; w < NW; w++) {
+            const int mine = (mode == 1) ? (dir ? ces[w] : cbs[w]) : (dir ? cew[w] : cbw[w]);
+            int prio = 0;
+            if (srch.sort_nodes >= 2) {
+                const int other = (mode == 1) ? (dir ? cbs[w] : ces[w]) : (dir ? cbw[w] : cew[w]);
+                if (srch.sort_crit == 1) prio = mine;
+                else if (srch.sort_crit == 2) prio = mine - other;
+                else if (mine <= 0) prio = 99999;
+                else if (valid[w]) {
+                    // the row is flagged already (pruned cells hold -j-1): the
+                    // reference sorts before pruning, so take the job itself
+                    const int u = cell_job(row[w]);
+                    prio = dir ? weak_back_idle(T, S, u) : weak_front_idle(T, S, u);
+                }
+            }
+            const unsigned long long lo = (unsigned)prio ^ 0x80000000u;   // signed order as unsigned
+            key[w] = srch.sort_nodes == 3 ? lo : ((unsigned long long)(unsigned)mine << 32) | lo;
+        }
+        sort_cells(S.rowj, k, key[0], NW > 1 ? key[NW - 1] : 0ull, row[0], NW > 1 ? row[NW - 1] : 0);
 #pragma unroll
         for (int w = 0; w < NW; w++)
             if (valid[w]) row[w] = (signed char)S.rowj[w * 32 + lane];

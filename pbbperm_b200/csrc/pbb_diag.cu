@@ -9,6 +9,7 @@
 #include <string.h>
 
 #include "../../include/pbbperm_diag.h"
+#include "pbb_devguard.h"
 
 #define DIAG_CHAINS 8
 
@@ -37,6 +38,7 @@ __global__ void pbb_diag_int32_kernel(int iters, int seed, int* out)
 extern "C" int pbb_diag_int32_peak(int32_t device, double* gops, double* seconds)
 {
     if (!gops) return -1;
+    pbbh::DeviceGuard keep_callers_device;
     if (cudaSetDevice(device) != cudaSuccess) return -3;
     int sms = 0;
     cudaDeviceGetAttribute(&sms, cudaDevAttrMultiProcessorCount, device);

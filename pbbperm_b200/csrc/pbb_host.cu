@@ -8,9 +8,11 @@
 #include <chrono>
 #include <climits>
 #include <string>
+#include <thread>
 #include <vector>
 
 #include "pbb_types.h"
+#include "pbb_devguard.h"
 #include "pbb_launch.h"
 #include "pbb_tables.h"
 #include "../../include/pbbperm.h"
@@ -126,7 +128,55 @@ struct pbb_engine {
     int32_t ub = INT32_MAX;
     double slice_s = 2.0;
     int select_budget = 4096;
+    int max_rounds = INT_MAX;      // explorer loop rounds per launch
+    SampleBuf* sample_d = nullptr; // node sampling (diagnostic), NULL when off
+    int* sample_rec = nullptr;
+    int sample_stride = 0;
+    double wait_limit_s = -1.0;    // host wait per window: < 0 window + 60 s, 0 unbounded
+    bool pending = false;          // a window whose wait ran out is still on the stream
 };
+
+namespace {
+
+// Wait for `ev` with a host-side deadline: PBB_E_TIMEOUT when it has not
+// completed after limit_s seconds (limit_s <= 0: wait without limit).  Polls
+// with a short sleep so that the waiting thread does not spin a core.
+int wait_event(cudaEvent_t ev, double limit_s)
+{
+    if (limit_s <= 0) {
+        CK(cudaEventSynchronize(ev));
+        return PBB_OK;
+    }
+    const auto t0 = std::chrono::steady_clock::now();
+    unsigned sleep_us = 20;
+    while (true) {
+        const cudaError_t q = cudaEventQuery(ev);
+        if (q == cudaSuccess) return PBB_OK;
+        if (q != cudaErrorNotReady) return cuda_fail(q, "exploration window");
+        const double el = std::chrono::duration<double>(std::chrono::steady_clock::now() - t0).count();
+        if (el > limit_s) return PBB_E_TIMEOUT;
+        std::this_thread::sleep_for(std::chrono::microseconds(sleep_us));
+        sleep_us = std::min(2 * sleep_us, 500u);
+    }
+}
+
+// Account a window whose host wait ran out: it ends by its own device-time
+// budget, so this blocks for at most the rest of that budget.
+int settle(pbb_engine* e)
+{
+    if (!e->pending) return PBB_OK;
+    CK(cudaEventSynchronize(e->ev1));
+    float ms = 0.f;
+    CK(cudaEventElapsedTime(&ms, e->ev0, e->ev1));
+    e->dev_seconds += ms * 1e-3;
+    int active = 0;
+    CK(cudaMemcpy(&active, &e->ctl->active, sizeof(int), cudaMemcpyDeviceToHost));
+    e->done = (active == 0);
+    e->pending = false;
+    return PBB_OK;
+}
+
+}  // namespace
 
 extern "C" {
 
@@ -140,21 +190,58 @@ void pbb_config_default(pbb_config* c)
     c->johnson_mode = 0;
     c->early_stop_johnson = 0;
     c->sorted_dfs = 0;
+    c->sorting_criterion = 1;
     c->nb_ivms = 16384;
     c->device = 0;
 }
 
 const char* pbb_last_error(void) { return g_err.c_str(); }
 
-static int check_config(const pbb_config* c)
+}  // extern "C"
+
+namespace pbbh {
+// Search settings every entry point accepts (engine and pool).
+// earlyStopJohnson: a child's Johnson scan stops once its running maximum
+// exceeds the incumbent (bound_fsp_strong.cpp:154-158); that child is pruned
+// either way, so node counts do not change -- except with the Johnson bound
+// choosing the side by MaxSum (boundingMode 1, adaptiveBranchingMode 1),
+// where the pruned children's partial values enter the choice and, in the
+// reference, depend on each thread's machine-pair success history
+// (:112-122): that combination is rejected.
+int check_search(const pbb_config* c)
 {
     if (c->bounding_mode < 0 || c->bounding_mode > 2) return fail(PBB_E_INVAL, "boundingMode must be 0, 1 or 2");
     const int b = c->branching_mode;
     if (!(b == -3 || b == -2 || b == -1 || b == 1 || b == 2 || b == 3))
         return fail(PBB_E_INVAL, "adaptiveBranchingMode must be one of -3,-2,-1,1,2,3");
-    if (c->early_stop_johnson) return fail(PBB_E_UNSUPPORTED, "earlyStopJohnson=true is not supported");
-    if (c->sorted_dfs < 0 || c->sorted_dfs > 1)
-        return fail(PBB_E_UNSUPPORTED, "sortedDFS must be 0 or 1 (2-4 sort by idle-time priorities, not computed here)");
+    if (c->early_stop_johnson && c->bounding_mode == 1 && b == 1)
+        return fail(PBB_E_UNSUPPORTED, "earlyStopJohnson=true with boundingMode=1 and MaxSum branching is not "
+                                       "supported (the side choice would depend on a thread's pair-order history)");
+    if (c->sorted_dfs < 0 || c->sorted_dfs > 4) return fail(PBB_E_INVAL, "sortedDFS must be in 0..4");
+    if (c->sorted_dfs >= 2) {
+        // the sibling priorities of chooseChildrenSet (ivm_bound.cpp:506-544)
+        const int k = c->sorting_criterion;
+        if (k == 4)
+            return fail(PBB_E_UNSUPPORTED, "sortingCriterion=4 is not supported: the reference's completeSchedule "
+                                           "writes past the node's free jobs, so its priorities are not defined");
+        if (k < 1 || k > 4) return fail(PBB_E_INVAL, "sortingCriterion must be 1, 2 or 3 with sortedDFS >= 2");
+        if (k == 3 && c->bounding_mode == 1)
+            return fail(PBB_E_UNSUPPORTED, "sortingCriterion=3 with boundingMode=1 is not supported: the reference "
+                                           "reads an unset Johnson idle time for children with one free job");
+        if (k == 2 && c->bounding_mode == 1 && c->early_stop_johnson)
+            return fail(PBB_E_UNSUPPORTED, "sortingCriterion=2 with boundingMode=1 and earlyStopJohnson=true is not "
+                                           "supported: the priority would read a pruned side's partial bound");
+    }
+    return PBB_OK;
+}
+}  // namespace pbbh
+
+extern "C" {
+
+static int check_config(const pbb_config* c)
+{
+    const int rc = pbbh::check_search(c);
+    if (rc) return rc;
     if (c->nb_ivms < 1 || c->nb_ivms > (1 << 22)) return fail(PBB_E_INVAL, "nbIVMs must be in [1, 4194304]");
     return PBB_OK;
 }
@@ -162,6 +249,7 @@ static int check_config(const pbb_config* c)
 int pbb_engine_destroy(pbb_engine* e)
 {
     if (!e) return PBB_OK;
+    pbbh::DeviceGuard keep_callers_device;
     cudaSetDevice(e->dev);
     if (e->st) cudaStreamSynchronize(e->st);
     e->di.release();
@@ -169,6 +257,8 @@ int pbb_engine_destroy(pbb_engine* e)
     cudaFree(e->line); cudaFree(e->state); cudaFree(e->bestcost); cudaFree(e->qval); cudaFree(e->qseq);
     cudaFree(e->ub_d); cudaFree(e->root_d); cudaFree(e->ival_d); cudaFree(e->ctl); cudaFree(e->group_d);
     cudaFree(e->ngroups_d);
+    cudaFree(e->sample_d);
+    cudaFree(e->sample_rec);
     if (e->ev0) cudaEventDestroy(e->ev0);
     if (e->ev1) cudaEventDestroy(e->ev1);
     if (e->st) cudaStreamDestroy(e->st);
@@ -184,6 +274,7 @@ static int engine_create(const pbb_instance* inst, const pbb_config* cfg, pbb_en
     rc = build_tables(inst, cfg->johnson_mode, e->H);
     if (rc) return rc;
     e->dev = cfg->device;
+    pbbh::DeviceGuard keep_callers_device;
     CK(cudaSetDevice(e->dev));
     CK(cudaStreamCreateWithFlags(&e->st, cudaStreamNonBlocking));
     CK(cudaEventCreate(&e->ev0));
@@ -226,6 +317,8 @@ static int engine_create(const pbb_instance* inst, const pbb_config* cfg, pbb_en
     g.search.branch_mode = cfg->branching_mode;
     g.search.find_all = cfg->find_all ? 1 : 0;
     g.search.sort_nodes = cfg->sorted_dfs;
+    g.search.sort_crit = cfg->sorting_criterion;
+    g.search.early_stop = cfg->early_stop_johnson ? 1 : 0;
     g.ivm.count = B;
     g.ivm.npad = npad;
     g.ivm.mat = e->mat;
@@ -269,6 +362,7 @@ int pbb_engine_create(const pbb_instance* inst, const pbb_config* cfg, pbb_engin
 static int start_impl(pbb_engine* e, int32_t ub, const int32_t* root_perm, const int32_t* pos, const int32_t* end)
 {
     if (!e) return fail(PBB_E_INVAL, "engine is NULL");
+    pbbh::DeviceGuard keep_callers_device;
     CK(cudaSetDevice(e->dev));
     const int n = e->H.n;
     std::vector<int> root(PBB_MAX_N, 0);
@@ -296,6 +390,7 @@ static int start_impl(pbb_engine* e, int32_t ub, const int32_t* root_perm, const
     CK(pbbl::launch_reset(e->group_d, 1, e->ub_d, e->st));
     CK(pbbl::launch_root(e->nw, e->group_d, 1, e->root_d, e->ival_d, PBB_MAX_N, e->root_smem, e->st));
     CK(cudaStreamSynchronize(e->st));
+    e->pending = false;
     GroupCtl c;
     CK(cudaMemcpy(&c, e->ctl, sizeof(c), cudaMemcpyDeviceToHost));
     e->started = true;
@@ -320,6 +415,7 @@ int pbb_init_from_fac(pbb_engine* e, int32_t ub, const int32_t* root_perm, int32
     const int B = e->cfg.nb_ivms;
     if (nb_intervals < 1 || nb_intervals > B) return fail(PBB_E_INVAL, "nb_intervals must be in [1, nb_ivms]");
     if (ub < 0) return fail(PBB_E_INVAL, "ub must be >= 0");
+    pbbh::DeviceGuard keep_callers_device;
     CK(cudaSetDevice(e->dev));
     const int n = e->H.n;
     std::vector<int> root(PBB_MAX_N, 0);
@@ -358,6 +454,7 @@ int pbb_init_from_fac(pbb_engine* e, int32_t ub, const int32_t* root_perm, int32
         err = pbbl::launch_root(e->nw, e->group_d, 1, e->root_d, ival_d, PBB_MAX_N, e->root_smem, e->st,
                                 nb_intervals, ids_d);
     if (!err) err = cudaStreamSynchronize(e->st);
+    if (!err) e->pending = false;
     cudaFree(ival_d);
     cudaFree(ids_d);
     if (err) return fail(PBB_E_CUDA, std::string("init_from_fac: ") + cudaGetErrorString(err));
@@ -375,7 +472,12 @@ int pbb_get_intervals(pbb_engine* e, int32_t max_intervals, int32_t* pos, int32_
 {
     if (!e || !e->started) return fail(PBB_E_INVAL, "engine not started");
     if (!nb_intervals) return fail(PBB_E_INVAL, "nb_intervals is NULL");
+    pbbh::DeviceGuard keep_callers_device;
     CK(cudaSetDevice(e->dev));
+    {
+        const int rs = settle(e);
+        if (rs) return rs;
+    }
     CK(cudaStreamSynchronize(e->st));
     const int B = e->cfg.nb_ivms, n = e->H.n;
     std::vector<int> st(B);
@@ -423,25 +525,116 @@ int pbb_get_intervals(pbb_engine* e, int32_t max_intervals, int32_t* pos, int32_
 int pbb_set_ub(pbb_engine* e, int32_t ub)
 {
     if (!e || !e->started) return fail(PBB_E_INVAL, "engine not started");
+    pbbh::DeviceGuard keep_callers_device;
     CK(cudaSetDevice(e->dev));
+    {
+        const int rs = settle(e);
+        if (rs) return rs;
+    }
     CK(pbbl::launch_lower_ub(e->group_d, 0, ub, e->st));
     CK(cudaStreamSynchronize(e->st));
+    return PBB_OK;
+}
+
+int pbb_set_wait_limit(pbb_engine* e, double seconds)
+{
+    if (!e) return fail(PBB_E_INVAL, "engine is NULL");
+    e->wait_limit_s = seconds;
+    return PBB_OK;
+}
+
+int pbb_diag_set_step_limits(pbb_engine* e, int32_t select_budget, int32_t max_rounds)
+{
+    if (!e) return fail(PBB_E_INVAL, "engine is NULL");
+    if (select_budget < 1 || max_rounds < 1) return fail(PBB_E_INVAL, "limits must be >= 1");
+    e->select_budget = select_budget;
+    e->max_rounds = max_rounds;
+    return PBB_OK;
+}
+
+int pbb_diag_sample_nodes(pbb_engine* e, int32_t capacity, int32_t rate_log2)
+{
+    if (!e) return fail(PBB_E_INVAL, "engine is NULL");
+    if (capacity < 0 || rate_log2 < 0 || rate_log2 > 30) return fail(PBB_E_INVAL, "bad sampling parameters");
+    pbbh::DeviceGuard keep_callers_device;
+    CK(cudaSetDevice(e->dev));
+    {
+        const int rs = settle(e);
+        if (rs) return rs;
+    }
+    CK(cudaStreamSynchronize(e->st));
+    cudaFree(e->sample_d);
+    cudaFree(e->sample_rec);
+    e->sample_d = nullptr;
+    e->sample_rec = nullptr;
+    e->group.sample = nullptr;
+    if (capacity > 0) {
+        e->sample_stride = PBB_SAMPLE_HDR + 5 * e->H.n;
+        const size_t bytes = sizeof(int) * (size_t)capacity * e->sample_stride;
+        CK(cudaMalloc(&e->sample_rec, bytes));
+        CK(cudaMalloc(&e->sample_d, sizeof(SampleBuf)));
+        CK(cudaMemsetAsync(e->sample_rec, 0, bytes, e->st));
+        SampleBuf sb;
+        sb.count = 0;
+        sb.cap = (unsigned)capacity;
+        sb.rate_mask = (1u << rate_log2) - 1u;
+        sb.stride = e->sample_stride;
+        sb.rec = e->sample_rec;
+        CK(cudaMemcpyAsync(e->sample_d, &sb, sizeof(sb), cudaMemcpyHostToDevice, e->st));
+        e->group.sample = e->sample_d;
+    }
+    CK(cudaMemcpyAsync(e->group_d, &e->group, sizeof(DevGroup), cudaMemcpyHostToDevice, e->st));
+    CK(cudaStreamSynchronize(e->st));
+    return PBB_OK;
+}
+
+int pbb_diag_get_samples(pbb_engine* e, int32_t max_records, int32_t* out, int32_t* count)
+{
+    if (!e || !count) return fail(PBB_E_INVAL, "NULL argument");
+    *count = 0;
+    if (!e->sample_d) return PBB_OK;
+    pbbh::DeviceGuard keep_callers_device;
+    CK(cudaSetDevice(e->dev));
+    {
+        const int rs = settle(e);
+        if (rs) return rs;
+    }
+    CK(cudaStreamSynchronize(e->st));
+    SampleBuf sb;
+    CK(cudaMemcpy(&sb, e->sample_d, sizeof(sb), cudaMemcpyDeviceToHost));
+    const int have = (int)std::min(sb.count, sb.cap);
+    const int k = std::min(have, std::max(0, (int)max_records));
+    if (k > 0) {
+        if (!out) return fail(PBB_E_INVAL, "out is NULL");
+        CK(cudaMemcpy(out, e->sample_rec, sizeof(int) * (size_t)k * e->sample_stride, cudaMemcpyDeviceToHost));
+    }
+    *count = max_records > 0 ? k : have;
     return PBB_OK;
 }
 
 int pbb_explore(pbb_engine* e, double seconds, int32_t* done)
 {
     if (!e || !e->started) return fail(PBB_E_INVAL, "engine not started");
+    pbbh::DeviceGuard keep_callers_device;
     CK(cudaSetDevice(e->dev));
+    int rc = settle(e);
+    if (rc) return rc;
     if (!e->done) {
         // a launch never runs unbounded: at most 120 s of device time per window
         const double win = (seconds > 0 && seconds < 120.0) ? seconds : 120.0;
         const unsigned long long budget = (unsigned long long)(win * 1e9);
         CK(cudaEventRecord(e->ev0, e->st));
-        CK(pbbl::launch_explore(e->nw, e->group_d, e->ngroups_d, e->ctas, e->warps, e->smem, budget, INT_MAX,
-                                e->select_budget, e->st, e->cfg.sorted_dfs));
+        const int variant = e->sample_d ? 2 : ((e->cfg.sorted_dfs || e->cfg.early_stop_johnson) ? 1 : 0);
+        CK(pbbl::launch_explore(e->nw, e->group_d, e->ngroups_d, e->ctas, e->warps, e->smem, budget, e->max_rounds,
+                                e->select_budget, e->st, variant));
         CK(cudaEventRecord(e->ev1, e->st));
-        CK(cudaStreamSynchronize(e->st));
+        rc = wait_event(e->ev1, e->wait_limit_s < 0 ? win + 60.0 : e->wait_limit_s);
+        if (rc == PBB_E_TIMEOUT) {
+            e->pending = true;
+            return fail(PBB_E_TIMEOUT, "the exploration window did not end within the host wait limit; it ends by "
+                                       "its own device-time budget and the next call accounts for it");
+        }
+        if (rc) return rc;
         float ms = 0.f;
         CK(cudaEventElapsedTime(&ms, e->ev0, e->ev1));
         e->dev_seconds += ms * 1e-3;
@@ -456,7 +649,12 @@ int pbb_explore(pbb_engine* e, double seconds, int32_t* done)
 int pbb_get_result(pbb_engine* e, pbb_result* out)
 {
     if (!e || !out) return fail(PBB_E_INVAL, "NULL argument");
+    pbbh::DeviceGuard keep_callers_device;
     CK(cudaSetDevice(e->dev));
+    {
+        const int rs = settle(e);
+        if (rs) return rs;
+    }
     CK(cudaStreamSynchronize(e->st));
     GroupCtl c;
     CK(cudaMemcpy(&c, e->ctl, sizeof(c), cudaMemcpyDeviceToHost));
@@ -547,6 +745,7 @@ static int bound_children_impl(const pbb_instance* inst, int32_t johnson_mode, i
             seen[j] = 1;
         }
     }
+    pbbh::DeviceGuard keep_callers_device;
     CK(cudaSetDevice(device));
     cudaStream_t st;
     CK(cudaStreamCreateWithFlags(&st, cudaStreamNonBlocking));
@@ -606,7 +805,12 @@ static int bound_children_impl(const pbb_instance* inst, int32_t johnson_mode, i
 int pbb_work_counters(pbb_engine* e, pbb_work* out)
 {
     if (!e || !out) return fail(PBB_E_INVAL, "NULL argument");
+    pbbh::DeviceGuard keep_callers_device;
     CK(cudaSetDevice(e->dev));
+    {
+        const int rs = settle(e);
+        if (rs) return rs;
+    }
     CK(cudaStreamSynchronize(e->st));
     GroupCtl c;
     CK(cudaMemcpy(&c, e->ctl, sizeof(c), cudaMemcpyDeviceToHost));
@@ -624,6 +828,7 @@ int pbb_work_counters(pbb_engine* e, pbb_work* out)
     out->direct_free_jobs = c.jdirect_free;
     out->explorers = e->cfg.nb_ivms;
     out->warps = e->warps * e->ctas;
+    out->status = (int32_t)c.status;
     return PBB_OK;
 }
 

@@ -7,6 +7,7 @@
 //   pbb_bound_kernel     batched children bounds of given nodes (LB parity API)
 #include <cuda_runtime.h>
 #include <stdint.h>
+#include <climits>
 #include "pbb_types.h"
 #include "pbb_device.cuh"
 #include "pbb_launch.h"
@@ -319,8 +320,52 @@ __device__ __forceinline__ int select_node(const DevGroup& G, const CtaTables& T
     return 2;
 }
 
+// Node sampling (SampleBuf): claim a record for the node about to be bounded
+// when the hash of (explorer, the warp's decomposed count) falls under the
+// group's rate, and write its header and fixed jobs; NULL when not sampled or
+// when the buffer is full (recording never waits).
+template <int NW>
+__device__ __forceinline__ int* sample_slot(const DevGroup& G, const WarpScratch& S, const Ivm<NW>& R, int id, int f,
+                                            int b, int best, unsigned long long step)
+{
+    SampleBuf* sb = G.sample;
+    int slot = -1;
+    if (lane_id() == 0 && sb) {
+        unsigned h = (unsigned)id * 0x9E3779B1u ^ (unsigned)step * 0x85EBCA77u;
+        h ^= h >> 15;
+        h *= 0x2C1B3C6Du;
+        h ^= h >> 12;
+        h *= 0x297A2D39u;
+        h ^= h >> 15;
+        if ((h & sb->rate_mask) == 0) {
+            const unsigned c = atomicAdd(&sb->count, 1u);
+            if (c < sb->cap) slot = (int)c;
+        }
+    }
+    slot = __shfl_sync(FULLMASK, slot, 0);
+    if (slot < 0) return nullptr;
+    int* rec = sb->rec + (size_t)slot * sb->stride;
+    const int n = G.inst.n, L = R.line;
+    int fc = 0, bc = 0;
+    build_lists<NW>(S, R, L, fc, bc);
+    int* sch = rec + PBB_SAMPLE_HDR;
+    for (int i = lane_id(); i < f; i += 32) sch[i] = S.fjob[i];
+    for (int i = lane_id(); i < b; i += 32) sch[n - 1 - i] = S.bjob[i];
+    if (lane_id() == 0) {
+        rec[0] = id;
+        rec[1] = L;
+        rec[2] = f - 1;
+        rec[3] = n - b;
+        rec[5] = best;
+        rec[6] = n - L;
+        rec[7] = 0;
+    }
+    __syncwarp();
+    return rec;
+}
+
 // Bound and prune the node selected at R.line and write its row back.
-template <int NW, int SORT>
+template <int NW, int SORT, int SAMPLE>
 __device__ __forceinline__ void bound_current(const DevGroup& G, const CtaTables& T, const WarpScratch& S, int id,
                                               Ivm<NW>& R, int mode, int best, WarpCounters& C)
 {
@@ -328,8 +373,11 @@ __device__ __forceinline__ void bound_current(const DevGroup& G, const CtaTables
     const int f = front_count<NW>(R, L), b = L - f;
     partial_from_path(T, S, f, b, R.hf, R.hb, R.hr);
     const int prev = L > 0 ? vget<NW>(R.dir, L - 1) : 0;
+    int* rec = nullptr;
+    if (SAMPLE) rec = sample_slot<NW>(G, S, R, id, f, b, best, C.decomposed);
     NodeCounters nc = {0, 0, 0, 0, 0};
-    const int d = bound_and_prune<NW, SORT>(T, S, G.search, mode, R.row, T.n - L, f, b, L, prev, best, nc, true);
+    const int d = bound_and_prune<NW, SORT, SAMPLE>(T, S, G.search, mode, R.row, T.n - L, f, b, L, prev, best, nc,
+                                                    true, rec);
     vset<NW>(R.dir, L, d);
     store_row<NW>(G.ivm, id, L, R.row);
     C.simple += nc.simple;
@@ -656,10 +704,12 @@ __global__ void pbb_root_kernel(const DevGroup* groups, int ngroups, const int* 
 
 // Persistent explorer loop.  Warp w of a group serves explorers w, w+W, ...
 // (W = warps of the group).  Runs until no explorer of the group holds work,
-// or `budget_ns` of device time has passed, or `max_rounds` rounds.  SORT = 0
-// compiles the sortedDFS row sort out of the hot loop (SORT = 1 follows each
-// group's setting).
-template <int NW, int SORT>
+// or `budget_ns` of device time has passed, or `max_rounds` rounds.  VAR = 0
+// compiles the sortedDFS row sorts, the early Johnson exit and node sampling
+// out of the hot loop; VAR = 1 follows each group's sortedDFS and
+// earlyStopJohnson settings; VAR = 2 also records sampled nodes into the
+// group's SampleBuf.
+template <int NW, int VAR>
 __global__ void __launch_bounds__(32 * PBB_WARPS_MAX, 1)
 pbb_explore_kernel(const DevGroup* groups, const int* ngroups_d, int warps_per_cta, unsigned long long budget_ns,
                    int max_rounds, int select_budget)
@@ -743,7 +793,7 @@ pbb_explore_kernel(const DevGroup* groups, const int* ngroups_d, int warps_per_c
             if (gb < best) best = gb;
             try_share<NW>(G, id, R);
             const int r = select_node<NW>(G, T, S, id, R, best, C, select_budget);
-            if (r == 1) bound_current<NW, SORT>(G, T, S, id, R, mode, best, C);
+            if (r == 1) bound_current<NW, (VAR >= 1), (VAR == 2)>(G, T, S, id, R, mode, best, C);
             worked = true;
             if (r == 0) {
                 // interval exhausted: leave the pool of busy explorers (the
@@ -911,7 +961,7 @@ __global__ void pbb_bound_kernel(DevInstance I, int count, const int* sched, con
                             if (nc == q) { cjob[q] = j; cside[q] = c < k ? 0 : 1; }
                         nc++;
                         if (nc == PBB_DIRECT_MAX || c == 2 * k - 1) {
-                            if (T.posj) johnson_direct_masked<NW>(T, S, k, nc, cjob, cside);
+                            if (T.posj) johnson_direct_masked<NW>(T, S, k, nc, cjob, cside, INT_MAX);
                             else johnson_direct<NW>(T, S, um, nc, cjob, cside);
                             nc = 0;
                         }
@@ -944,19 +994,23 @@ namespace pbbl {
 
 int smem_bytes(int n, int m, int Ppad, int warps) { return pbb_smem_plan(n, m, Ppad, warps).total; }
 
-template <int NW, int SORT>
+template <int NW, int VAR>
 int explore_occupancy(int warps_per_cta, int smem)
 {
     int blocks = 0;
-    cudaFuncSetAttribute(pbb_explore_kernel<NW, SORT>, cudaFuncAttributeMaxDynamicSharedMemorySize, smem);
-    cudaOccupancyMaxActiveBlocksPerMultiprocessor(&blocks, pbb_explore_kernel<NW, SORT>, 32 * warps_per_cta, smem);
+    cudaFuncSetAttribute(pbb_explore_kernel<NW, VAR>, cudaFuncAttributeMaxDynamicSharedMemorySize, smem);
+    cudaOccupancyMaxActiveBlocksPerMultiprocessor(&blocks, pbb_explore_kernel<NW, VAR>, 32 * warps_per_cta, smem);
     return blocks;
 }
 
-int explore_ctas_per_sm(int nw, int warps_per_cta, int smem, int sort)
+int explore_ctas_per_sm(int nw, int warps_per_cta, int smem, int variant)
 {
-    if (nw == 1) return sort ? explore_occupancy<1, 1>(warps_per_cta, smem) : explore_occupancy<1, 0>(warps_per_cta, smem);
-    return sort ? explore_occupancy<2, 1>(warps_per_cta, smem) : explore_occupancy<2, 0>(warps_per_cta, smem);
+    if (nw == 1) {
+        if (variant == 2) return explore_occupancy<1, 2>(warps_per_cta, smem);
+        return variant ? explore_occupancy<1, 1>(warps_per_cta, smem) : explore_occupancy<1, 0>(warps_per_cta, smem);
+    }
+    if (variant == 2) return explore_occupancy<2, 2>(warps_per_cta, smem);
+    return variant ? explore_occupancy<2, 1>(warps_per_cta, smem) : explore_occupancy<2, 0>(warps_per_cta, smem);
 }
 
 cudaError_t launch_reset(const DevGroup* groups, int ngroups, const int* ub, cudaStream_t st)
@@ -986,28 +1040,29 @@ cudaError_t launch_lower_ub(const DevGroup* groups, int g, int ub, cudaStream_t 
     return cudaGetLastError();
 }
 
-template <int NW, int SORT>
+template <int NW, int VAR>
 cudaError_t explore_launch(const DevGroup* groups, const int* ngroups_d, int ctas, int warps_per_cta, int smem,
                            unsigned long long budget_ns, int max_rounds, int select_budget, cudaStream_t st)
 {
-    cudaFuncSetAttribute(pbb_explore_kernel<NW, SORT>, cudaFuncAttributeMaxDynamicSharedMemorySize, smem);
-    pbb_explore_kernel<NW, SORT><<<ctas, 32 * warps_per_cta, smem, st>>>(groups, ngroups_d, warps_per_cta, budget_ns,
-                                                                          max_rounds, select_budget);
+    cudaFuncSetAttribute(pbb_explore_kernel<NW, VAR>, cudaFuncAttributeMaxDynamicSharedMemorySize, smem);
+    pbb_explore_kernel<NW, VAR><<<ctas, 32 * warps_per_cta, smem, st>>>(groups, ngroups_d, warps_per_cta, budget_ns,
+                                                                         max_rounds, select_budget);
     return cudaGetLastError();
 }
 
 cudaError_t launch_explore(int nw, const DevGroup* groups, const int* ngroups_d, int ctas, int warps_per_cta, int smem,
-                           unsigned long long budget_ns, int max_rounds, int select_budget, cudaStream_t st, int sort)
+                           unsigned long long budget_ns, int max_rounds, int select_budget, cudaStream_t st,
+                           int variant)
 {
-    if (nw == 1)
-        return sort ? explore_launch<1, 1>(groups, ngroups_d, ctas, warps_per_cta, smem, budget_ns, max_rounds,
-                                           select_budget, st)
-                    : explore_launch<1, 0>(groups, ngroups_d, ctas, warps_per_cta, smem, budget_ns, max_rounds,
-                                           select_budget, st);
-    return sort ? explore_launch<2, 1>(groups, ngroups_d, ctas, warps_per_cta, smem, budget_ns, max_rounds,
-                                       select_budget, st)
-                : explore_launch<2, 0>(groups, ngroups_d, ctas, warps_per_cta, smem, budget_ns, max_rounds,
-                                       select_budget, st);
+#define PBB_EXPLORE(NW_, VAR_) \
+    explore_launch<NW_, VAR_>(groups, ngroups_d, ctas, warps_per_cta, smem, budget_ns, max_rounds, select_budget, st)
+    if (nw == 1) {
+        if (variant == 2) return PBB_EXPLORE(1, 2);
+        return variant ? PBB_EXPLORE(1, 1) : PBB_EXPLORE(1, 0);
+    }
+    if (variant == 2) return PBB_EXPLORE(2, 2);
+    return variant ? PBB_EXPLORE(2, 1) : PBB_EXPLORE(2, 0);
+#undef PBB_EXPLORE
 }
 
 cudaError_t launch_bound(int nw, const DevInstance& I, int count, const int* sched, const int* l1, const int* l2,

@@ -11,11 +11,13 @@ cudaError_t launch_reset(const DevGroup* groups, int ngroups, const int* ub, cud
 cudaError_t launch_root(int nw, const DevGroup* groups, int ngroups, const int* roots, const int* ivals,
                         int root_stride, int smem, cudaStream_t st, int per_group = 1, const int* ids = nullptr);
 cudaError_t launch_lower_ub(const DevGroup* groups, int g, int ub, cudaStream_t st);
-// sort = 1 when any listed group sorts its rows (sortedDFS = 1)
+// variant: 0 = no row sort, no early Johnson exit, no sampling (the hot
+// path); 1 = each group's sortedDFS / earlyStopJohnson settings; 2 = as 1 and
+// record sampled nodes (groups' SampleBuf)
 cudaError_t launch_explore(int nw, const DevGroup* groups, const int* ngroups_d, int ctas, int warps_per_cta, int smem,
                            unsigned long long budget_ns, int max_rounds, int select_budget, cudaStream_t st,
-                           int sort = 0);
-int explore_ctas_per_sm(int nw, int warps_per_cta, int smem, int sort = 0);
+                           int variant = 0);
+int explore_ctas_per_sm(int nw, int warps_per_cta, int smem, int variant = 0);
 cudaError_t launch_bound(int nw, const DevInstance& I, int count, const int* sched, const int* l1, const int* l2,
                          int* wb, int* we, int* sb, int* se, int* nweak, int* nstrong, unsigned int* status, int ctas,
                          int warps_per_cta, int smem, cudaStream_t st, int method = 0);

@@ -18,7 +18,12 @@
 //     word is cleared at the start of each call.  Calls whose work overlaps on
 //     the GPU (other host threads, other streams) race on the array and must
 //     not be issued concurrently; this entry point serialises its own host
-//     callers and waits for its stream before returning.
+//     callers and waits for its stream before returning;
+//   * the calling thread's current device is the same after the call as
+//     before it (the call selects `device` only while it runs);
+//   * the block shape shrinks (8 warps down to 1) until the tables fit the
+//     device's per-block shared memory; if even one warp does not fit, the
+//     call returns PBB_E_INVAL.
 #include <cuda_runtime.h>
 #include <stdint.h>
 #include <string.h>
@@ -28,6 +33,8 @@
 
 #include "pbb_types.h"
 #include "pbb_launch.h"
+#include "pbb_tables.h"
+#include "pbb_devguard.h"
 #include "../../include/pbbperm.h"
 
 #define PBB_NOALLOC_MAX_N 64
@@ -56,6 +63,7 @@ namespace {
 
 std::mutex g_noalloc_mutex;
 unsigned char* g_scratch_addr[PBB_NOALLOC_MAX_DEVICES];   // device address of the array, per device
+int g_smem_optin[PBB_NOALLOC_MAX_DEVICES];                 // per-block shared memory limit, per device
 
 // Host staging of the tables (static: building them allocates nothing).
 struct StagedTables {
@@ -66,43 +74,7 @@ struct StagedTables {
 };
 StagedTables g_stage;
 
-// Johnson keys and partition sort with the reference's tie order
-// (bounds/src/bound_fsp_strong.cpp:359-436), on fixed-size arrays.
-int na_grp[PBB_NOALLOC_MAX_N], na_val[PBB_NOALLOC_MAX_N];
-
-bool na_before(int x, int y)
-{
-    if (na_grp[x] != na_grp[y]) return na_grp[x] < na_grp[y];
-    return na_grp[x] == 1 ? na_val[x] < na_val[y] : na_val[x] > na_val[y];
-}
-
-bool na_after(int x, int y)
-{
-    if (na_grp[x] != na_grp[y]) return na_grp[x] > na_grp[y];
-    return na_grp[x] == 1 ? na_val[x] > na_val[y] : na_val[x] < na_val[y];
-}
-
-void na_sort(int* v, int lo, int hi)
-{
-    while (lo < hi) {
-        const int pivot = v[lo];
-        int i = lo - 1, j = hi + 1;
-        while (true) {
-            do { --j; } while (na_after(v[j], pivot));
-            do { ++i; } while (na_before(v[i], pivot));
-            if (i >= j) break;
-            const int t = v[i]; v[i] = v[j]; v[j] = t;
-        }
-        na_sort(v, lo, j);
-        lo = j + 1;
-    }
-}
-
 }  // namespace
-
-namespace pbbh {
-void set_error(const char* msg);   // pbb_host.cu: the message pbb_last_error() returns
-}
 
 static int na_fail(int code, const char* msg)
 {
@@ -110,66 +82,18 @@ static int na_fail(int code, const char* msg)
     return code;
 }
 
-// Tables of the instance (same contents as the engine's build_tables) into
-// the static host staging area.  Returns PBB_OK or PBB_E_*.
+// Tables of the instance into the static host staging area, with the same
+// builder (and so the same Johnson tie order) as the allocating entry points.
 static int na_build_tables(const pbb_instance* inst, int johnson_mode, int& P, int& Ppad)
 {
     const int n = inst->n_jobs, m = inst->n_machines;
-    const int32_t* p = inst->p;
-    for (int j = 0; j < n; j++) {
-        long s = 0;
-        for (int k = 0; k < m; k++) {
-            const int v = p[k * n + j];
-            if (v < 0 || v > 65535) return na_fail(PBB_E_INVAL, "processing times must be in [0, 65535]");
-            s += v;
-        }
-        if (s > 32767) return na_fail(PBB_E_INVAL, "a job's total processing time must be <= 32767");
-    }
-    memcpy(g_stage.p, p, sizeof(int) * n * m);
-    int* marr = g_stage.mt;
-    int* mdep = g_stage.mt + m;
-    for (int k = 0; k < m; k++) { marr[k] = INT_MAX; mdep[k] = INT_MAX; }
-    marr[0] = 0;
-    mdep[m - 1] = 0;
-    for (int j = 0; j < n; j++) {
-        int head = 0, tail = 0;
-        for (int k = 1; k < m; k++) { head += p[(k - 1) * n + j]; if (head < marr[k]) marr[k] = head; }
-        for (int k = m - 2; k >= 0; k--) { tail += p[(k + 1) * n + j]; if (tail < mdep[k]) mdep[k] = tail; }
-    }
-    P = 0;
-    for (int a = 0; a < m - 1; a++)
-        for (int b = a + 1; b < m; b++) {
-            if (johnson_mode == 1 && b < m - 1) continue;
-            if (johnson_mode == 2 && b != a + 1) continue;
-            P++;
-        }
+    const int rc = pbbt::check_times(inst->p, n, m);
+    if (rc != PBB_OK) return rc;
+    memcpy(g_stage.p, inst->p, sizeof(int) * n * m);
+    P = pbbt::count_pairs(m, johnson_mode);
     Ppad = (P + 31) / 32 * 32;
-    memset(g_stage.je, 0, sizeof(unsigned long long) * n * Ppad);
-    memset(g_stage.pm, 0, 2 * Ppad);
-    int order[PBB_NOALLOC_MAX_N], lag[PBB_NOALLOC_MAX_N];
-    int i = 0;
-    for (int a = 0; a < m - 1; a++)
-        for (int b = a + 1; b < m; b++) {
-            if (johnson_mode == 1 && b < m - 1) continue;
-            if (johnson_mode == 2 && b != a + 1) continue;
-            g_stage.pm[i] = (unsigned char)a;
-            g_stage.pm[Ppad + i] = (unsigned char)b;
-            for (int j = 0; j < n; j++) {
-                int l = 0;
-                for (int k = a + 1; k < b; k++) l += p[k * n + j];
-                lag[j] = l;
-                const int pa = p[a * n + j], pb = p[b * n + j];
-                na_grp[j] = pa < pb ? 1 : 2;
-                na_val[j] = (pa < pb ? pa : pb) + l;
-                order[j] = j;
-            }
-            na_sort(order, 0, n - 1);
-            for (int t = 0; t < n; t++) {
-                const int j = order[t];
-                g_stage.je[t * Ppad + i] = JE_PACK(j, p[a * n + j], p[b * n + j], lag[j]);
-            }
-            i++;
-        }
+    pbbt::TableSpans T{g_stage.je, nullptr, g_stage.pm, g_stage.pm + Ppad, g_stage.mt, g_stage.mt + m};
+    pbbt::fill_tables(inst->p, n, m, johnson_mode, Ppad, T);
     return PBB_OK;
 }
 
@@ -222,13 +146,23 @@ extern "C" int pbb_bound_children_noalloc(const pbb_instance* inst, int32_t john
     if (rc != PBB_OK) return rc;
     if (count == 0) return PBB_OK;
 
+    // the caller's current context comes back on every return path below
+    pbbh::DeviceGuard keep_callers_device;
     NA_CK(cudaSetDevice(device), "cudaSetDevice failed");
     unsigned char* base = g_scratch_addr[device];
     if (!base) {
         // set-up, once per device, with that device current
         NA_CK(cudaGetSymbolAddress((void**)&base, g_noalloc_scratch), "cudaGetSymbolAddress of the scratch failed");
+        NA_CK(cudaDeviceGetAttribute(&g_smem_optin[device], cudaDevAttrMaxSharedMemoryPerBlockOptin, device),
+              "device query failed");
         g_scratch_addr[device] = base;
     }
+    // block shape: the most warps (up to 8) whose tables and scratch fit the
+    // device's per-block shared memory
+    int warps = 8, smem = pbbl::smem_bytes(n, m, Ppad, warps);
+    while (warps > 1 && smem > g_smem_optin[device]) smem = pbbl::smem_bytes(n, m, Ppad, --warps);
+    if (smem > g_smem_optin[device])
+        return na_fail(PBB_E_INVAL, "instance tables do not fit in this device's shared memory");
     cudaStream_t st = static_cast<cudaStream_t>(stream);
     unsigned* status = reinterpret_cast<unsigned*>(base + NA_STATUS_OFF);
     unsigned long long* je = reinterpret_cast<unsigned long long*>(base + NA_JE_OFF);
@@ -257,8 +191,6 @@ extern "C" int pbb_bound_children_noalloc(const pbb_instance* inst, int32_t john
     I.p = pd; I.je = je; I.pm0 = pm; I.pm1 = pm + Ppad;
     I.min_arr = mt; I.min_dep = mt + m;
     I.posj = nullptr;   // method 0 (sweeps over all positions) needs no position table
-    const int warps = 8;
-    const int smem = pbbl::smem_bytes(n, m, Ppad, warps);
     int sms = 0;
     NA_CK(cudaDeviceGetAttribute(&sms, cudaDevAttrMultiProcessorCount, device), "device query failed");
     int ctas = (count + warps - 1) / warps;

@@ -12,9 +12,11 @@
 #include <climits>
 #include <deque>
 #include <map>
+#include <mutex>
 #include <vector>
 
 #include "pbb_types.h"
+#include "pbb_devguard.h"
 #include "pbb_launch.h"
 #include "pbb_tables.h"
 #include "../../include/pbbperm.h"
@@ -116,6 +118,9 @@ struct pbb_pool {
     int* ivals_d = nullptr;
     cudaGraphExec_t window = nullptr;
     std::vector<Slot> slots;
+    // the FIFO and the finished results are shared with submitting and
+    // polling threads; everything else belongs to the thread driving step()
+    std::mutex mu;
     std::deque<Request> queue;
     std::vector<pbb_pool_result> done;
     Arena alloc;
@@ -138,6 +143,7 @@ extern "C" void pbb_pool_config_default(pbb_pool_config* c)
 extern "C" int pbb_pool_destroy(pbb_pool* P)
 {
     if (!P) return PBB_OK;
+    pbbh::DeviceGuard keep_callers_device;
     cudaSetDevice(P->dev);
     if (P->st) cudaStreamSynchronize(P->st);
     if (P->window) cudaGraphExecDestroy(P->window);
@@ -207,6 +213,7 @@ int pool_create(const pbb_pool_config* in, pbb_pool* P)
     if (c.window_s > 120.0) return pfail(PBB_E_INVAL, "window_s must be <= 120");
     P->cfg = c;
     P->dev = c.device;
+    pbbh::DeviceGuard keep_callers_device;
     PCK(cudaSetDevice(P->dev), "cudaSetDevice failed");
     PCK(cudaStreamCreateWithFlags(&P->st, cudaStreamNonBlocking), "stream creation failed");
     P->nw = c.max_jobs <= 32 ? 1 : 2;
@@ -308,11 +315,8 @@ extern "C" int pbb_pool_submit(pbb_pool* P, const pbb_instance* inst, const pbb_
     pbb_config_default(&r.search);
     if (search) r.search = *search;
     const pbb_config& c = r.search;
-    if (c.bounding_mode < 0 || c.bounding_mode > 2) return pfail(PBB_E_INVAL, "boundingMode must be 0, 1 or 2");
-    if (!(c.branching_mode == -3 || c.branching_mode == -2 || c.branching_mode == -1 || c.branching_mode == 1 ||
-          c.branching_mode == 2 || c.branching_mode == 3))
-        return pfail(PBB_E_INVAL, "adaptiveBranchingMode must be one of -3,-2,-1,1,2,3");
-    if (c.early_stop_johnson) return pfail(PBB_E_UNSUPPORTED, "earlyStopJohnson=true is not supported");
+    const int rs = pbbh::check_search(&c);
+    if (rs) return rs;
     if (c.sorted_dfs)
         return pfail(PBB_E_UNSUPPORTED, "the pool explores with sortedDFS = 0 (the single-instance engine takes 1)");
     const int rc = pbbt::build_tables(inst, c.johnson_mode, r.H);
@@ -327,25 +331,36 @@ extern "C" int pbb_pool_submit(pbb_pool* P, const pbb_instance* inst, const pbb_
         r.root[i] = j;
     }
     r.ub = ub;
+    std::lock_guard<std::mutex> lock(P->mu);
     P->queue.push_back(std::move(r));
     return PBB_OK;
 }
 
 namespace {
 
-// admit queued instances while a slot and explorer memory are free (FIFO)
+// admit queued instances while a slot and explorer memory are free (FIFO);
+// submitters may push concurrently, so each request is moved out under the lock
 int admit(pbb_pool* P, std::vector<int>& admitted)
 {
     const int E = P->epw;
     const size_t bytes = explorer_block_bytes(E, P->npad);
-    while (!P->queue.empty()) {
+    while (true) {
         int s = -1;
         for (int i = 0; i < P->max_slots; i++)
             if (!P->slots[i].used) { s = i; break; }
         if (s < 0) break;
         size_t off = 0;
         if (!P->alloc.alloc(bytes, off)) break;
-        Request& r = P->queue.front();
+        Request r;
+        {
+            std::lock_guard<std::mutex> lock(P->mu);
+            if (P->queue.empty()) {
+                P->alloc.release(off, bytes);
+                break;
+            }
+            r = std::move(P->queue.front());
+            P->queue.pop_front();
+        }
         const pbbt::HostTables& H = r.H;
         unsigned char* tb = P->tables + (size_t)s * P->table_stride;
         PCK(cudaMemcpyAsync(tb + P->off_je, H.je.data(), H.je.size() * 8, cudaMemcpyHostToDevice, P->st), "upload");
@@ -378,12 +393,15 @@ int admit(pbb_pool* P, std::vector<int>& admitted)
         g.search.branch_mode = r.search.branching_mode;
         g.search.find_all = r.search.find_all ? 1 : 0;
         g.search.sort_nodes = r.search.sorted_dfs;
+        g.search.sort_crit = r.search.sorting_criterion;
+        // the pool's window graph runs the default explorer, which has no early
+        // Johnson exit: it leaves every decision unchanged, so it is not needed
+        g.search.early_stop = 0;
         carve_explorers(P->arena + off, E, P->npad, g.ivm);
         g.ctl = P->ctl + s;
         admitted.push_back(s);
         P->pending_ub.push_back(r.ub);
         P->pending_root.insert(P->pending_root.end(), r.root.begin(), r.root.end());
-        P->queue.pop_front();
     }
     return PBB_OK;
 }
@@ -393,6 +411,7 @@ int admit(pbb_pool* P, std::vector<int>& admitted)
 extern "C" int pbb_pool_step(pbb_pool* P, int32_t* resident, int32_t* queued)
 {
     if (!P) return pfail(PBB_E_INVAL, "pool is NULL");
+    pbbh::DeviceGuard keep_callers_device;
     PCK(cudaSetDevice(P->dev), "cudaSetDevice failed");
     std::vector<int> admitted;
     P->pending_ub.clear();
@@ -467,8 +486,10 @@ extern "C" int pbb_pool_step(pbb_pool* P, int32_t* resident, int32_t* queued)
         pr.status = (c.status & PBB_ST_BADINPUT) ? PBB_E_INVAL : PBB_OK;
         pbb_result& r = pr.result;
         const unsigned id = (unsigned)(c.best_key & 0xffffffffull);
-        r.complete = 1;
-        r.found = (c.found > 0 && id != 0xffffffffu && id < (unsigned)sl.explorers) ? 1 : 0;
+        // an instance the device flagged is neither complete nor solved
+        const bool ok = pr.status == PBB_OK;
+        r.complete = ok ? 1 : 0;
+        r.found = (ok && c.found > 0 && id != 0xffffffffu && id < (unsigned)sl.explorers) ? 1 : 0;
         r.cost = (int32_t)(c.best_key >> 32);
         r.n_jobs = sl.n;
         r.stats.decomposed = c.decomposed;
@@ -482,20 +503,27 @@ extern "C" int pbb_pool_step(pbb_pool* P, int32_t* resident, int32_t* queued)
                 "result read-back");
             for (int j = 0; j < sl.n; j++) r.perm[j] = buf[j];
         }
-        P->done.push_back(pr);
+        {
+            std::lock_guard<std::mutex> lock(P->mu);
+            P->done.push_back(pr);
+        }
         P->alloc.release(sl.off, sl.bytes);
         sl = Slot();
     }
     int res = 0;
     for (int s = 0; s < P->max_slots; s++) res += P->slots[s].used ? 1 : 0;
     if (resident) *resident = res;
-    if (queued) *queued = (int32_t)P->queue.size();
+    if (queued) {
+        std::lock_guard<std::mutex> lock(P->mu);
+        *queued = (int32_t)P->queue.size();
+    }
     return PBB_OK;
 }
 
 extern "C" int pbb_pool_poll(pbb_pool* P, pbb_pool_result* out, int32_t max, int32_t* count)
 {
     if (!P || (!out && max > 0)) return pfail(PBB_E_INVAL, "NULL argument");
+    std::lock_guard<std::mutex> lock(P->mu);
     const int k = std::min((int)P->done.size(), (int)std::max(0, max));
     for (int i = 0; i < k; i++) out[i] = P->done[i];
     P->done.erase(P->done.begin(), P->done.begin() + k);
@@ -541,6 +569,7 @@ extern "C" int pbb_batch_solve(const pbb_instance* inst, int32_t count, const pb
     int32_t res = 0, q = count;
     std::vector<pbb_pool_result> out(count);
     int got_total = 0;
+    int first_bad = PBB_OK;     // first per-instance error, returned after the batch
     while (!rc && (res > 0 || q > 0 || got_total < count)) {
         rc = pbb_pool_step(P, &res, &q);
         if (rc) break;
@@ -549,10 +578,12 @@ extern "C" int pbb_batch_solve(const pbb_instance* inst, int32_t count, const pb
         for (int i = 0; i < got; i++) {
             const int64_t t = out[i].tag;
             if (t >= 0 && t < count) results[t] = out[i].result;
+            if (out[i].status != PBB_OK && first_bad == PBB_OK) first_bad = out[i].status;
         }
         got_total += got;
         if (res == 0 && q == 0) break;
     }
     pbb_pool_destroy(P);
+    if (!rc && first_bad != PBB_OK) return pfail(first_bad, "the device rejected an instance of the batch");
     return rc;
 }

@@ -15,9 +15,7 @@
 #define IVM_ACTIVE 2          // holds a non-empty interval
 
 // status bits written by kernels (never traps)
-#define PBB_ST_BADINPUT 1u
-#define PBB_ST_QUEUE 2u
-#define PBB_ST_SPIN 4u
+#define PBB_ST_BADINPUT 1u    // a node or instance the kernel rejected
 
 // Packed Johnson entry for (pair i, Johnson position t):
 //   bits 0..15 p[m0][job], 16..31 p[m1][job], 32..39 job id, 40..63 lag[i][job]
@@ -49,7 +47,10 @@ struct DevSearch {
     int bound_mode;    // 0 weak, 1 strong, 2 weak then strong
     int branch_mode;   // -3,-2,-1 fixed; 1 MaxSum, 2 MinBranch, 3 MinMin
     int find_all;
-    int sort_nodes;    // [bb] sortedDFS: 0 reverse the row on a side change, 1 sort it by cost
+    int sort_nodes;    // [bb] sortedDFS: 0 reverse the row on a side change, 1 sort it by cost,
+                       //      2 and 4 by (cost, priority), 3 by priority
+    int sort_crit;     // [bb] sortingCriterion (sortedDFS >= 2): 1 cost, 2 cost minus the other side's, 3 idle time
+    int early_stop;    // [bb] earlyStopJohnson: a child's Johnson scan may stop once it exceeds the incumbent
 };
 
 // Per-group control block (device memory).
@@ -92,6 +93,25 @@ struct DevIvms {
 
 #define PBB_PATH_INTS 96   // ints per path level: heads, tails, free loads, 32 machines each
 
+// Opt-in record of nodes the explorer bounded, as it bounded them (LB parity
+// of the explorer's own bound code).  A node is recorded when a hash of
+// (explorer id, the warp's decomposed count) has its low bits clear under
+// rate_mask, until `cap` records are taken; recording never waits.
+// Record layout (ints): PBB_SAMPLE_HDR header
+//   [0] explorer id  [1] line  [2] limit1  [3] limit2  [4] side chosen
+//   [5] incumbent at bounding  [6] free jobs k  [7] 0
+// then five arrays of n: schedule (front jobs, free jobs, back jobs as the
+// reference's node->schedule), weak LB front / back and Johnson LB front /
+// back by job id (0 = not evaluated).
+#define PBB_SAMPLE_HDR 8
+struct SampleBuf {
+    unsigned count;        // records claimed (may exceed cap; only cap are written)
+    unsigned cap;
+    unsigned rate_mask;
+    int stride;            // ints per record: PBB_SAMPLE_HDR + 5 n
+    int* rec;
+};
+
 struct DevGroup {
     DevInstance inst;
     DevSearch search;
@@ -99,6 +119,7 @@ struct DevGroup {
     GroupCtl* ctl;
     int first_cta;         // CTAs [first_cta, first_cta + ctas) work on this group
     int ctas;
+    SampleBuf* sample;     // NULL unless node sampling is armed
 };
 
 // Dynamic shared memory layout of one CTA (host and device agree).

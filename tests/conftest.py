@@ -9,12 +9,6 @@ if ROOT not in sys.path:
     sys.path.insert(0, ROOT)
 GOLDEN = os.path.join(ROOT, "tests", "golden")
 
-# the 20x20 seed-1 instance (Johnson bound, UB = optimum 2352): reference
-# multicore counters measured with oracle/_ref/bbJ, 8 threads
-CONFIG2 = dict(n=20, m=20, seed=1, opt=2352, decomposed=12616547, johnson_bounds=25431709,
-               simple_bounds=236462768, leaves=0)
-
-
 def pytest_configure(config):
     config.addinivalue_line("markers", "gpu: needs a CUDA device (B200)")
 
@@ -40,3 +34,14 @@ def search_golden():
 @pytest.fixture(scope="session")
 def sorted_golden():
     return load_golden("sorted_golden.json")
+
+
+@pytest.fixture(scope="session")
+def config2_golden(search_golden):
+    """The second configuration (20x20 seed 1, weak then Johnson, UB = optimum
+    2352): the reference multicore's counters, written into
+    search_golden.json by `make_golden.py --big-only`."""
+    big = [r for r in search_golden["runs"] if r.get("big")]
+    if not big:
+        pytest.skip("search_golden.json has no config-2 entry (make_golden.py --big-only)")
+    return big[0]

@@ -17,8 +17,13 @@ B&B `bb` / `bbJ`).  Instances come from the project's seeded generator
                       sortedDFS 0 and 1: the exploration order decides when the
                       bound improves, so the counters pin the order of the children.
 
-Usage: python tests/golden/make_golden.py [--big] [--sorted-only]   (--big adds
-the 20x20 seed-1 instance, several CPU-minutes of reference time)
+Usage: python tests/golden/make_golden.py [--big] [--big-only] [--sorted-only] [--early-stop-only]
+       [--priorities-only]
+(--big adds the 20x20 seed-1 instance of the second configuration, several
+CPU-minutes of reference time; --big-only runs just that case and replaces the
+`big` entry of search_golden.json, keeping the other runs; --early-stop-only
+replaces the earlyStopJohnson = true runs of both search fixtures;
+--priorities-only replaces the sortedDFS 2-4 runs of sorted_golden.json)
 """
 import json
 import os
@@ -142,12 +147,7 @@ def make_search(big=False):
     runs.append(dict(n=20, m=5, seed=0, ub=None, bounding_mode=0, branching_mode=3, find_all=False,
                      opt=r["best"], perm=r["perm"]))
     if big:
-        p = synthetic_instance(1, 20, 20)
-        opt = 2352
-        r = run_reference_bb(p, ub=opt, bound_mode=2, branch_mode=3, threads=8, johnson=True, timeout=20000)
-        runs.append(dict(n=20, m=20, seed=1, opt=opt, ub=opt, bounding_mode=2, branching_mode=3, find_all=False,
-                         decomposed=r["decomposed"], johnson_bounds=r["johnson_bounds"],
-                         simple_bounds=r["simple_bounds"], leaves=r["leaves"], big=True))
+        runs.append(big_run())
     else:
         old = os.path.join(HERE, "search_golden.json")
         if os.path.exists(old):
@@ -155,6 +155,108 @@ def make_search(big=False):
                 runs += [r for r in json.load(f)["runs"] if r.get("big")]
     with open(os.path.join(HERE, "search_golden.json"), "w") as f:
         json.dump(dict(source="reference multicore B&B (oracle/_ref/bb, bbJ), 8 threads", runs=runs), f, indent=0)
+
+
+def big_run():
+    """The second configuration: 20 jobs x 20 machines (seed 1), weak then
+    Johnson bound, MinMin, UB = its optimum 2352 (found by the reference from
+    UB = +inf), 8 reference threads: the node counters are deterministic."""
+    p = synthetic_instance(1, 20, 20)
+    opt = 2352
+    r = run_reference_bb(p, ub=opt, bound_mode=2, branch_mode=3, threads=8, johnson=True, timeout=20000)
+    print("big", r, flush=True)
+    return dict(n=20, m=20, seed=1, opt=opt, ub=opt, bounding_mode=2, branching_mode=3, find_all=False,
+                decomposed=r["decomposed"], johnson_bounds=r["johnson_bounds"],
+                simple_bounds=r["simple_bounds"], leaves=r["leaves"], big=True)
+
+
+EARLY_STOP_MODES = [(2, 3), (2, 1), (2, 2), (1, 3), (1, 2)]
+
+
+def make_early_stop():
+    """Reference runs with earlyStopJohnson = true (its default): at UB =
+    optimum on 8 threads (deterministic counters), and on ONE thread from
+    UB = +inf with sortedDFS 0 and 1.  Appended to search_golden.json /
+    sorted_golden.json with early_stop = true, replacing earlier such runs.
+    boundingMode 1 with MaxSum is left out: there the reference's counters
+    depend on each thread's machine-pair success history."""
+    path = os.path.join(HERE, "search_golden.json")
+    with open(path) as f:
+        g = json.load(f)
+    runs = [r for r in g["runs"] if not r.get("early_stop")]
+    for n, m, seed in SEARCH_CASES[:6]:
+        p = synthetic_instance(seed, n, m)
+        opt = Oracle(p).solve(INF, bound_mode=2)["best"]
+        for bm, br in EARLY_STOP_MODES:
+            r = run_reference_bb(p, ub=opt, bound_mode=bm, branch_mode=br, threads=8, johnson=True,
+                                 early_stop=True, timeout=600)
+            runs.append(dict(n=n, m=m, seed=seed, opt=opt, ub=opt, bounding_mode=bm, branching_mode=br,
+                             find_all=False, early_stop=True, decomposed=r["decomposed"],
+                             johnson_bounds=r["johnson_bounds"], simple_bounds=r["simple_bounds"],
+                             leaves=r["leaves"]))
+            print("early-stop run", n, m, seed, bm, br, r["decomposed"], flush=True)
+    g["runs"] = runs
+    with open(path, "w") as f:
+        json.dump(g, f, indent=0)
+    path = os.path.join(HERE, "sorted_golden.json")
+    with open(path) as f:
+        g = json.load(f)
+    runs = [r for r in g["runs"] if not r.get("early_stop")]
+    for n, m, seed in SORTED_CASES[:2]:
+        p = synthetic_instance(seed, n, m)
+        for bm, br in [(2, 3), (1, 2)]:
+            for sd in (0, 1):
+                r = run_reference_bb(p, ub=None, bound_mode=bm, branch_mode=br, threads=1, johnson=True,
+                                     sorted_dfs=sd, early_stop=True, timeout=600)
+                runs.append(dict(n=n, m=m, seed=seed, p=p.tolist(), bounding_mode=bm, branching_mode=br,
+                                 sorted_dfs=sd, early_stop=True, best=r["best"], decomposed=r["decomposed"],
+                                 johnson_bounds=r["johnson_bounds"], simple_bounds=r["simple_bounds"],
+                                 leaves=r["leaves"]))
+    g["runs"] = runs
+    with open(path, "w") as f:
+        json.dump(g, f, indent=0)
+
+
+PRIORITY_MODES = [(0, 3), (2, 3), (2, 1), (1, 2), (2, -3)]
+
+
+def make_priorities():
+    """sortedDFS 2-4 with sortingCriterion 1-3 on ONE reference thread from
+    UB = +inf: rows sorted by (first cost, priority) or by the priority
+    (ivm_bound.cpp:338-370, priorities :506-544).  Appended to
+    sorted_golden.json with their sorting_criterion, replacing earlier such
+    runs.  Left out: criterion 3 with boundingMode 1 (the reference reads an
+    unset Johnson idle time for children with one free job) and criterion 4
+    (completeSchedule writes past the node's free block)."""
+    path = os.path.join(HERE, "sorted_golden.json")
+    with open(path) as f:
+        g = json.load(f)
+    runs = [r for r in g["runs"] if r["sorted_dfs"] <= 1]
+    for n, m, seed in SORTED_CASES:
+        p = synthetic_instance(seed, n, m)
+        for bm, br in PRIORITY_MODES:
+            for sd in (2, 3, 4):
+                for crit in (1, 2, 3):
+                    if bm == 1 and crit == 3:
+                        continue
+                    r = run_reference_bb(p, ub=None, bound_mode=bm, branch_mode=br, threads=1, johnson=(bm != 0),
+                                         sorted_dfs=sd, sorting_criterion=crit, timeout=600)
+                    runs.append(dict(n=n, m=m, seed=seed, p=p.tolist(), bounding_mode=bm, branching_mode=br,
+                                     sorted_dfs=sd, sorting_criterion=crit, best=r["best"],
+                                     decomposed=r["decomposed"], johnson_bounds=r["johnson_bounds"],
+                                     simple_bounds=r["simple_bounds"], leaves=r["leaves"]))
+    g["runs"] = runs
+    with open(path, "w") as f:
+        json.dump(g, f, indent=0)
+
+
+def make_big_only():
+    path = os.path.join(HERE, "search_golden.json")
+    with open(path) as f:
+        g = json.load(f)
+    g["runs"] = [r for r in g["runs"] if not r.get("big")] + [big_run()]
+    with open(path, "w") as f:
+        json.dump(g, f, indent=0)
 
 
 def make_sorted():
@@ -177,6 +279,18 @@ def make_sorted():
 if __name__ == "__main__":
     if not oracle.reference_available():
         sys.exit("build the reference checker first: python oracle/build_ref.py")
+    if "--priorities-only" in sys.argv:
+        make_priorities()
+        print("sortedDFS 2-4 runs written")
+        sys.exit(0)
+    if "--early-stop-only" in sys.argv:
+        make_early_stop()
+        print("early-stop runs written")
+        sys.exit(0)
+    if "--big-only" in sys.argv:
+        make_big_only()
+        print("search_golden.json: big run replaced")
+        sys.exit(0)
     if "--sorted-only" not in sys.argv:
         if "--search-only" not in sys.argv:
             make_bounds()

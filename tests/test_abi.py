@@ -46,11 +46,18 @@ def test_invalid_instances_rejected_before_cuda():
 def test_unsupported_options_rejected():
     p = synthetic_instance(0, 10, 4)
     with pytest.raises(pb.PbbError) as e:
-        pb.Engine(p, pb.Config(earlyStopJohnson=True))
+        # early Johnson exit where pruned children's values choose the side
+        pb.Engine(p, pb.Config(earlyStopJohnson=True, boundingMode=1, adaptiveBranchingMode=1))
     assert e.value.code == pb.PBB_E_UNSUPPORTED
     with pytest.raises(pb.PbbError) as e:
-        pb.Engine(p, pb.Config(sortedDFS=2))           # sorts by idle-time priorities
+        pb.Engine(p, pb.Config(sortedDFS=2, sortingCriterion=4))    # undefined in the reference
     assert e.value.code == pb.PBB_E_UNSUPPORTED
+    with pytest.raises(pb.PbbError) as e:
+        pb.Engine(p, pb.Config(sortedDFS=3, sortingCriterion=3, boundingMode=1))
+    assert e.value.code == pb.PBB_E_UNSUPPORTED
+    with pytest.raises(pb.PbbError) as e:
+        pb.Engine(p, pb.Config(sortedDFS=5))
+    assert e.value.code == pb.PBB_E_INVAL
     with pytest.raises(pb.PbbError) as e:
         pb.Engine(p, pb.Config(adaptiveBranchingMode=4))
     assert e.value.code == pb.PBB_E_INVAL

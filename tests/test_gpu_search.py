@@ -3,7 +3,6 @@ UB = optimum, exact optima re-verified from the returned permutation."""
 import numpy as np
 import pytest
 
-from conftest import CONFIG2
 from oracle import Oracle
 import pbbperm_b200 as pb
 from pbbperm_b200.instances import synthetic_instance
@@ -21,16 +20,29 @@ def solve(p, ub, ivms=1024, **cfg):
 def test_sorted_dfs_sequential_vs_reference_golden(sorted_golden):
     """One explorer from UB = +inf explores in the reference's sequential order,
     so its counters, which depend on when the bound improves, must equal the
-    reference's single-thread run, with the rows reversed (sortedDFS = 0) or
-    sorted by the chosen side's bound (sortedDFS = 1)."""
+    reference's single-thread run, with the rows reversed (sortedDFS = 0),
+    sorted by the chosen side's bound (1), by (bound, priority) (2, 4) or by
+    the priority (3), with and without the early Johnson exit."""
     for r in sorted_golden["runs"]:
         p = np.array(r["p"], np.int32)
         got = solve(p, 2**31 - 1, ivms=1, boundingMode=r["bounding_mode"],
-                    adaptiveBranchingMode=r["branching_mode"], sortedDFS=r["sorted_dfs"])
+                    adaptiveBranchingMode=r["branching_mode"], sortedDFS=r["sorted_dfs"],
+                    sortingCriterion=r.get("sorting_criterion", 1), earlyStopJohnson=r.get("early_stop", False))
         assert got["complete"] and got["found"] and got["cost"] == r["best"]
         for k in KEYS:
             assert got[k] == r[k], (r["seed"], r["bounding_mode"], r["branching_mode"], r["sorted_dfs"], k,
                                     got[k], r[k])
+
+
+@pytest.mark.parametrize("sorted_dfs,crit", [(2, 2), (3, 3), (4, 1)])
+def test_priority_sorts_at_the_optimum_many_explorers(sorted_dfs, crit):
+    """At UB = optimum the node set does not depend on the order: sortedDFS
+    2-4 with 16384 explorers give the oracle's counters."""
+    p = synthetic_instance(24, 13, 20)
+    want = Oracle(p).solve(1803, bound_mode=2, sorted_dfs=sorted_dfs, sorting_criterion=crit)
+    got = solve(p, 1803, ivms=16384, boundingMode=2, sortedDFS=sorted_dfs, sortingCriterion=crit)
+    for k in KEYS:
+        assert got[k] == want[k], (k, got[k], want[k])
 
 
 @pytest.mark.parametrize("ivms", [64, 16384])
@@ -50,7 +62,7 @@ def test_counters_vs_reference_golden(search_golden):
             continue
         p = synthetic_instance(r["seed"], r["n"], r["m"])
         got = solve(p, r["ub"], boundingMode=r["bounding_mode"], adaptiveBranchingMode=r["branching_mode"],
-                    findAll=r["find_all"])
+                    findAll=r["find_all"], earlyStopJohnson=r.get("early_stop", False))
         assert got["complete"]
         for k in KEYS:
             assert got[k] == r[k], (r, k, got[k])
@@ -139,10 +151,10 @@ def test_root_permutation_respected():
         assert got[k] == want[k]
 
 
-def test_config2_20x20_johnson_ub_opt():
+def test_config2_20x20_johnson_ub_opt(config2_golden):
     """20 jobs x 20 machines (seed 1), weak+Johnson bound, 16384 explorers,
     UB = optimum 2352: decomposed-node count equals the reference's."""
-    c = CONFIG2
+    c = config2_golden
     p = synthetic_instance(c["seed"], c["n"], c["m"])
     got = solve(p, c["opt"], ivms=16384, boundingMode=2)
     assert got["complete"]

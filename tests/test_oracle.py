@@ -62,14 +62,15 @@ def test_oracle_search_vs_golden(search_golden):
 
 
 def test_oracle_sorted_dfs_vs_golden(sorted_golden):
-    """sortedDFS 0 and 1 from UB = +inf on one reference thread: the counters
-    depend on the order children are explored in, so they pin the row sort
-    (gnome sort by the chosen side's first cost) and the row reversal."""
+    """sortedDFS 0-4 from UB = +inf on one reference thread: the counters
+    depend on the order children are explored in, so they pin the row
+    reversal, the sort by the chosen side's first cost and the sorts by
+    (cost, priority) and by priority for sortingCriterion 1-3."""
     KEYS = ("decomposed", "johnson_bounds", "simple_bounds", "leaves")
     for r in sorted_golden["runs"]:
         p = np.array(r["p"], np.int32)
         got = Oracle(p).solve(2**31 - 1, bound_mode=r["bounding_mode"], branch_mode=r["branching_mode"],
-                              sorted_dfs=r["sorted_dfs"])
+                              sorted_dfs=r["sorted_dfs"], sorting_criterion=r.get("sorting_criterion", 1))
         assert got["best"] == r["best"]
         for k in KEYS:
             assert got[k] == r[k], (r["seed"], r["bounding_mode"], r["branching_mode"], r["sorted_dfs"], k)
