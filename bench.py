@@ -14,8 +14,9 @@ and table build), root + unfold, one window, result read-back, destroy.
   python bench.py [--gpus N] [--steps K] [--warmup W] [--window S] [--impl reference]
 
 Under torchrun each rank explores its own slice of the permutation space
-(factoradic sub-interval of the root level) and the ranks exchange the best
-makespan (a 4-byte MIN all-reduce) between windows.
+(factoradic sub-interval of the root level); between windows the ranks
+exchange the best makespan (a 4-byte MIN all-reduce) and an idle rank takes
+half of the busiest rank's intervals (pbbperm_b200.distributed.rebalance).
 """
 import argparse
 import json
@@ -157,16 +158,18 @@ class ClockSampler:
 # ---------------------------------------------------------------------------
 def rank_slice(n, rank, world):
     """(pos, end) factoradic vectors of rank's share of the first level:
-    the n root cells are split into contiguous blocks, one per rank."""
+    the n root cells are split into contiguous blocks, one per rank.  A rank
+    left without a cell (world > n) gets an empty interval (pos after end)."""
     if world == 1:
         return None
     per = [n // world + (1 if r < n % world else 0) for r in range(world)]
     lo = sum(per[:rank])
     hi = lo + per[rank] - 1
+    rest = [n - 1 - i for i in range(1, n)]
     if per[rank] == 0:
-        return None
+        return [n - 1] + [0] * (n - 1), [0] + rest
     pos = [lo] + [0] * (n - 1)
-    end = [hi] + [n - 1 - i for i in range(1, n)]
+    end = [hi] + rest
     return pos, end
 
 
@@ -208,14 +211,21 @@ def run_ours(args):
         t1 = eng.result()
         return t1["decomposed"] - t0["decomposed"], t1["device_seconds"] - t0["device_seconds"], done, t1
 
-    def exchange_ub(res):
+    from pbbperm_b200 import distributed as pdist
+    root = list(range(N_JOBS))
+
+    def exchange_ub(res, done=False):
+        """Between windows: the incumbent (MIN all-reduce), then rebalancing
+        -- an idle rank takes half of the busiest rank's intervals."""
         if dist is None:
             return
-        eng.set_ub(exchange_incumbent(dist, res["cost"], "cuda"))
+        best = exchange_incumbent(dist, res["cost"], "cuda")
+        eng.set_ub(best)
+        pdist.rebalance(dist, eng, N_JOBS, best, root, device="cuda", done=done)
 
     for _ in range(args.warmup):
-        _, _, _, res = window()
-        exchange_ub(res)
+        _, _, done, res = window()
+        exchange_ub(res, done)
     torch.cuda.synchronize()
     if dist:
         dist.barrier()
@@ -231,7 +241,7 @@ def run_ours(args):
             dev_s += ds
             launches += 1          # the explorer kernel (idle queue persists across launches)
             steps_done += 1
-            exchange_ub(res)
+            exchange_ub(res, done)
         torch.cuda.synchronize()
         wall = time.perf_counter() - wall0
     if dist:

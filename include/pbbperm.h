@@ -16,12 +16,16 @@
  *                       gpubb.h:161; gpubb::interruptExploration gpubb.h:35;
  *                       matrix_controller::interruptExploration
  *                       multicore/src/matrix_controller.cpp:459-462)
+ *   pbb_save_checkpoint / pbb_load_checkpoint
+ *                       works::save / works::init_infile (distributed/src/works.cpp:61-90,172-190)
  *   pbb_start_interval / pbb_init_from_fac / pbb_get_intervals
  *                       gpubb::initAtInterval / initFromFac / getIntervals
  *                       (gpubb.h:155,171,172; gpubb.cu:1190-1310)
  *   pbb_bound_children  bound_abstract::boundChildren + bornes_calculer
  *                       (bounds/include/bound_abstract.h:15-26) for a batch of nodes
  *   pbb_neh             fastNEH::runNEH initial upper bound (heuristic/src/fastNEH.cpp:230-243)
+ *   pbb_neh_batch       the same on the device for many instances (fastNEH.cpp:100-243)
+ *   pbb_ig_batch        IG::runIG iterated greedy on the device (heuristic/src/IG.cpp:341-416)
  *   pbb_engine_destroy  gpubb::~gpubb (gpubb.h:27; gpubb.cu:75)
  */
 #ifndef PBBPERM_H
@@ -42,6 +46,12 @@ extern "C" {
 
 #define PBB_MAX_JOBS 64
 #define PBB_MAX_MACHINES 32
+
+/* Initial bound value asking for NEH computed on the device (pbb_start,
+ * pbb_solve, pbb_pool_submit, pbb_batch_solve): the search starts from the
+ * NEH makespan, the reference's heuristic start ([initial] ub = 1,
+ * common/src/pbab.cpp:196-200), with no host round trip. */
+#define PBB_UB_NEH (-1)
 
 /* Instance: n_jobs x n_machines processing times, row-major machine-major
  * (p[k * n_jobs + j] = time of job j on machine k), the order of the
@@ -90,6 +100,9 @@ typedef struct pbb_result {
     int32_t perm[PBB_MAX_JOBS]; /* best permutation when found */
     pbb_stats stats;
     double device_seconds;      /* device time of the exploration kernels */
+    int32_t has_perm;           /* 1: perm holds a schedule of makespan `cost` -- a leaf found it, or
+                                   the search started from PBB_UB_NEH and did not improve on NEH */
+    int32_t pad;
 } pbb_result;
 
 typedef struct pbb_engine pbb_engine;
@@ -140,6 +153,22 @@ int pbb_get_intervals(pbb_engine* e, int32_t max_intervals, int32_t* pos, int32_
  * device-time budget, and the next call on the engine waits for it and
  * accounts for its work, so counters and intervals stay consistent. */
 int pbb_set_wait_limit(pbb_engine* e, double seconds);
+
+/* Checkpoint file of a search between windows, in the form the reference's
+ * distributed master saves (works::save, distributed/src/works.cpp:172-190;
+ * read back by works::init_infile :61-90): root solution, simple-bound
+ * count, best solution, then one work whose intervals are the explorers'
+ * (pbb_get_intervals) as decimal permutation indices (fact_work::VectToBigint,
+ * distributed/src/fact_work.cpp:74-87).  pbb_load_checkpoint resumes such a
+ * file in an engine of the same instance (pbb_init_from_fac with the best
+ * makespan as the bound; the stored best schedule is reported when no leaf
+ * improves it) and returns the stored bound count (may be NULL). */
+int pbb_save_checkpoint(pbb_engine* e, const char* path);
+int pbb_load_checkpoint(pbb_engine* e, const char* path, uint64_t* saved_simple_bounds);
+/* A factoradic vector (n digits, digit i in [0, n-i)) as the decimal index
+ * sum_i d_i (n-1-i)!, and back (indices below n!). */
+int pbb_fact_to_decimal(int32_t n, const int32_t* digits, char* out, int32_t out_len);
+int pbb_decimal_to_fact(int32_t n, const char* decimal, int32_t* digits);
 
 /* Lower the incumbent to `ub` (a bound found by another solver; no
  * permutation is attached): solution::updateCost (common/src/solution.cpp:44-56). */
@@ -234,6 +263,24 @@ int pbb_bound_children_noalloc(const pbb_instance* inst, int32_t johnson_mode, i
 /* NEH upper bound: jobs by decreasing total time, each inserted at the first
  * position of least partial makespan (host code). */
 int pbb_neh(const pbb_instance* inst, int32_t* perm, int32_t* cost);
+
+/* The same NEH on the device for `count` instances at once (one warp each,
+ * Taillard's head/tail insertion: fastNEH::insertJobInBestPosition,
+ * heuristic/src/fastNEH.cpp:206-220); results equal pbb_neh's.  perms has a
+ * stride of PBB_MAX_JOBS per instance. */
+int pbb_neh_batch(const pbb_instance* inst, int32_t count, int32_t device, int32_t* perms, int32_t* costs);
+
+/* Iterated greedy from the NEH schedule on the device, one warp per instance
+ * (IG::runIG, heuristic/src/IG.cpp:341-416): per round, 2 to 5 jobs removed
+ * from a shuffled prefix of the middle-out visit order (:120-160), each put
+ * back at its best position (:229-255), first-improvement insertion moves
+ * within sqrt(n) places (localSearchKI :567-612), and the temperature
+ * acceptance of 0.2 x mean time / 10 (:258-274) in the integer form
+ * T / (T + delta).  Every random decision comes from the splitmix64 stream
+ * seeded with seed + instance index, so a run is reproducible.  Same output
+ * layout as pbb_neh_batch; the makespan never exceeds NEH's. */
+int pbb_ig_batch(const pbb_instance* inst, int32_t count, int32_t device, int32_t iterations, uint64_t seed,
+                 int32_t* perms, int32_t* costs);
 
 #ifdef __cplusplus
 }

@@ -68,6 +68,8 @@ def lib():
         L.orc_solve_interval.argtypes = [ctypes.c_void_p, ctypes.POINTER(_OrcCfg), ctypes.c_int, _i32p, _i32p,
                                          _i32p, ctypes.POINTER(_OrcResult), _i32p]
         L.orc_neh.argtypes = [ctypes.c_void_p, _i32p]
+        L.orc_ig.argtypes = [ctypes.c_void_p, ctypes.c_int, ctypes.c_int, ctypes.c_int, ctypes.c_int,
+                             ctypes.c_uint64, _i32p]
         L.orc_synthetic_instance.argtypes = [ctypes.c_uint64, ctypes.c_int, ctypes.c_int, ctypes.c_int,
                                              ctypes.c_int, _i32p]
         L.orc_taillard_instance.argtypes = [ctypes.c_long, ctypes.c_int, ctypes.c_int, _i32p]
@@ -156,6 +158,12 @@ class Oracle:
     def neh(self):
         perm = np.zeros(self.n, np.int32)
         c = lib().orc_neh(self._h, _ptr(perm))
+        return c, perm
+
+    def ig(self, iterations, seed, destruct=2, destruct_max=5, ls_passes=64):
+        """The engine's seeded iterated greedy, restated (see orc_ig)."""
+        perm = np.zeros(self.n, np.int32)
+        c = lib().orc_ig(self._h, iterations, destruct, destruct_max, ls_passes, seed, _ptr(perm))
         return c, perm
 
     def solve(self, ub, bound_mode=2, branch_mode=3, find_all=False, root=None, node_limit=0, pos=None, end=None,

@@ -766,3 +766,128 @@ int orc_neh(const orc_inst *I, int *perm)
     memcpy(perm, seq, sizeof(int) * n);
     return partial_makespan(I, perm, n);
 }
+
+/* ------------------------------------------------------------------------ */
+/* Iterated greedy, the checker of the device IG                             */
+/* ------------------------------------------------------------------------ */
+
+/* The reference's IG (heuristic/src/IG.cpp:341-416) draws its decisions from
+ * std::random_device, so no run of it can be reproduced.  The engine's IG
+ * follows the same steps with a seeded splitmix64 stream; this is a plain
+ * restatement of that definition, evaluating every candidate by a direct
+ * makespan, used to check the device kernel draw for draw:
+ *   start: NEH (orc_neh);
+ *   round: d = perturbation (2, growing to 5 after rejections, :393-396)
+ *     destruction (:120-160): r uniform in [d, n], the first r entries of the
+ *       middle-out visit order (:33-45) shuffled (Fisher-Yates, j uniform in
+ *       [i, r-1]), the jobs at the first d shuffled positions removed in draw
+ *       order, the rest compacted;
+ *     construction (:229-255): each removed job at the first position of least
+ *       makespan;
+ *     local search (localSearchKI :567-612): passes over the visit order; the
+ *       job at position i goes to the first best place within isqrt(n) of i;
+ *       a strict improvement is kept and starts a new pass; at most
+ *       `ls_passes` passes;
+ *     acceptance (:258-274): one draw u (the high 32 bits of the next value);
+ *       kept when not worse, or when u < 2^32 T / (T + 1000 delta) with
+ *       T = 20 x total time / (n m), i.e. 1000 x 0.2 x mean time / 10. */
+static uint64_t ig_next(uint64_t *s)
+{
+    *s += 0x9E3779B97F4A7C15ull;
+    uint64_t z = *s;
+    z = (z ^ (z >> 30)) * 0xBF58476D1CE4E5B9ull;
+    z = (z ^ (z >> 27)) * 0x94D049BB133111EBull;
+    return z ^ (z >> 31);
+}
+
+static int ig_range(uint64_t *s, int a, int b)
+{
+    return a + (int)(((unsigned __int128)ig_next(s) * (uint64_t)(b - a + 1)) >> 64);
+}
+
+/* first position in [lo, hi] of least makespan for x inserted into seq[0..len) */
+static int ig_best_pos(const orc_inst *I, const int *seq, int len, int x, int lo, int hi, int *cost)
+{
+    int trial[ORC_MAXN], best = INT_MAX, bpos = lo;
+    for (int q = lo; q <= hi; q++) {
+        for (int i = 0, t = 0; i <= len; i++) trial[i] = (i == q) ? x : seq[t++];
+        int c = partial_makespan(I, trial, len + 1);
+        if (c < best) { best = c; bpos = q; }
+    }
+    *cost = best;
+    return bpos;
+}
+
+static void ig_insert(int *seq, int len, int pos, int x)
+{
+    for (int i = len; i > pos; i--) seq[i] = seq[i - 1];
+    seq[pos] = x;
+}
+
+int orc_ig(const orc_inst *I, int iterations, int destruct, int destruct_max, int ls_passes, uint64_t seed,
+           int *perm)
+{
+    int n = I->n, m = I->m;
+    int cur[ORC_MAXN], best[ORC_MAXN], seq[ORC_MAXN], vo[ORC_MAXN], order[ORC_MAXN], removed[ORC_MAXN];
+    int cur_cost = orc_neh(I, cur);
+    int best_cost = cur_cost;
+    memcpy(best, cur, sizeof(int) * n);
+    long long sum = 0;
+    for (int i = 0; i < n * m; i++) sum += I->p[i];
+    long long temp1000 = 20 * sum / ((long long)n * m);
+    int start = n / 2, ind = 0;
+    for (int i = start; i < n; i++) { vo[ind] = i; ind += 2; }
+    ind = 1;
+    for (int i = start - 1; i >= 0; i--) { vo[ind] = i; ind += 2; }
+    int kmax = 1;
+    while ((kmax + 1) * (kmax + 1) <= n) kmax++;
+    uint64_t rs = seed;
+    int perturb = destruct;
+    for (int it = 0; it < iterations && n >= 3; it++) {
+        int d = perturb < n - 1 ? perturb : n - 1;
+        memcpy(seq, cur, sizeof(int) * n);
+        int r = ig_range(&rs, d, n);
+        for (int i = 0; i < r; i++) order[i] = vo[i];
+        for (int i = 0; i < r - 1; i++) {
+            int j = ig_range(&rs, i, r - 1);
+            int t = order[i]; order[i] = order[j]; order[j] = t;
+        }
+        unsigned char gone[ORC_MAXN];
+        memset(gone, 0, sizeof(gone));
+        for (int i = 0; i < d; i++) { removed[i] = seq[order[i]]; gone[order[i]] = 1; }
+        int w = 0;
+        for (int i = 0; i < n; i++) if (!gone[i]) seq[w++] = seq[i];
+        int len = n - d, c;
+        for (int i = 0; i < d; i++) {
+            int pos = ig_best_pos(I, seq, len, removed[i], 0, len, &c);
+            ig_insert(seq, len, pos, removed[i]);
+            len++;
+        }
+        int cost = partial_makespan(I, seq, n);
+        for (int pass = 0; pass < ls_passes; pass++) {
+            int improved = 0;
+            for (int j = 0; j < n && !improved; j++) {
+                int i = vo[j], x = seq[i];
+                for (int q = i; q < n - 1; q++) seq[q] = seq[q + 1];
+                int lo = i - kmax > 0 ? i - kmax : 0, hi = i + kmax < n - 1 ? i + kmax : n - 1;
+                int pos = ig_best_pos(I, seq, n - 1, x, lo, hi, &c);
+                if (c < cost) { ig_insert(seq, n - 1, pos, x); cost = c; improved = 1; }
+                else ig_insert(seq, n - 1, i, x);
+            }
+            if (!improved) break;
+        }
+        long long delta = (long long)cost - cur_cost;
+        uint64_t u = ig_next(&rs) >> 32;
+        int accept = delta <= 0 || u < ((uint64_t)temp1000 << 32) / (uint64_t)(temp1000 + 1000 * delta);
+        if (accept) {
+            memcpy(cur, seq, sizeof(int) * n);
+            cur_cost = cost;
+            perturb = destruct;
+        } else {
+            perturb = perturb + 1 > destruct_max ? destruct : perturb + 1;
+        }
+        if (cost < best_cost) { best_cost = cost; memcpy(best, seq, sizeof(int) * n); }
+    }
+    memcpy(perm, best, sizeof(int) * n);
+    return best_cost;
+}

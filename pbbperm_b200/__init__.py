@@ -30,6 +30,7 @@ PBB_E_TIMEOUT = -4
 PBB_E_UNSUPPORTED = -5
 MAX_JOBS = 64
 INF = 2**31 - 1
+UB_NEH = -1          # initial bound: NEH computed on the device
 
 _i32p = ctypes.POINTER(ctypes.c_int32)
 
@@ -62,7 +63,7 @@ class _Stats(ctypes.Structure):
 class _Result(ctypes.Structure):
     _fields_ = [("complete", ctypes.c_int32), ("found", ctypes.c_int32), ("cost", ctypes.c_int32),
                 ("n_jobs", ctypes.c_int32), ("perm", ctypes.c_int32 * MAX_JOBS), ("stats", _Stats),
-                ("device_seconds", ctypes.c_double)]
+                ("device_seconds", ctypes.c_double), ("has_perm", ctypes.c_int32), ("pad", ctypes.c_int32)]
 
 
 class _Work(ctypes.Structure):
@@ -108,12 +109,19 @@ def lib():
         L.pbb_bound_children.argtypes = [ctypes.POINTER(_Instance), ctypes.c_int32, ctypes.c_int32, ctypes.c_int32,
                                          _i32p, _i32p, _i32p, _i32p, _i32p, _i32p, _i32p, _i32p, _i32p]
         L.pbb_neh.argtypes = [ctypes.POINTER(_Instance), _i32p, _i32p]
+        L.pbb_neh_batch.argtypes = [ctypes.POINTER(_Instance), ctypes.c_int32, ctypes.c_int32, _i32p, _i32p]
+        L.pbb_ig_batch.argtypes = [ctypes.POINTER(_Instance), ctypes.c_int32, ctypes.c_int32, ctypes.c_int32,
+                                   ctypes.c_uint64, _i32p, _i32p]
         L.pbb_start_interval.argtypes = [ctypes.c_void_p, ctypes.c_int32, _i32p, _i32p, _i32p]
         L.pbb_init_from_fac.argtypes = [ctypes.c_void_p, ctypes.c_int32, _i32p, ctypes.c_int32, _i32p, _i32p, _i32p]
         L.pbb_get_intervals.argtypes = [ctypes.c_void_p, ctypes.c_int32, _i32p, _i32p, _i32p,
                                         ctypes.POINTER(ctypes.c_int32)]
         L.pbb_set_ub.argtypes = [ctypes.c_void_p, ctypes.c_int32]
         L.pbb_set_wait_limit.argtypes = [ctypes.c_void_p, ctypes.c_double]
+        L.pbb_save_checkpoint.argtypes = [ctypes.c_void_p, ctypes.c_char_p]
+        L.pbb_load_checkpoint.argtypes = [ctypes.c_void_p, ctypes.c_char_p, ctypes.POINTER(ctypes.c_uint64)]
+        L.pbb_fact_to_decimal.argtypes = [ctypes.c_int32, _i32p, ctypes.c_char_p, ctypes.c_int32]
+        L.pbb_decimal_to_fact.argtypes = [ctypes.c_int32, ctypes.c_char_p, _i32p]
         L.pbb_diag_set_step_limits.argtypes = [ctypes.c_void_p, ctypes.c_int32, ctypes.c_int32]
         L.pbb_diag_sample_nodes.argtypes = [ctypes.c_void_p, ctypes.c_int32, ctypes.c_int32]
         L.pbb_diag_get_samples.argtypes = [ctypes.c_void_p, ctypes.c_int32, _i32p, ctypes.POINTER(ctypes.c_int32)]
@@ -180,7 +188,7 @@ class Config:
 
 def _result(r):
     n = r.n_jobs
-    return dict(complete=bool(r.complete), found=bool(r.found), cost=r.cost,
+    return dict(complete=bool(r.complete), found=bool(r.found), cost=r.cost, has_perm=bool(r.has_perm),
                 perm=np.array(r.perm[:n], dtype=np.int32),
                 decomposed=r.stats.decomposed, johnson_bounds=r.stats.johnson_bounds,
                 simple_bounds=r.stats.simple_bounds, leaves=r.stats.leaves, steals=r.stats.steals,
@@ -261,6 +269,17 @@ class Engine:
     def set_ub(self, ub):
         """Lower the incumbent to a bound found elsewhere (no permutation)."""
         _check(lib().pbb_set_ub(self._h, int(ub)))
+
+    def save_checkpoint(self, path):
+        """Write the search's state between windows in the reference's
+        works::save form (root, bound count, incumbent, intervals)."""
+        _check(lib().pbb_save_checkpoint(self._h, os.fsencode(path)))
+
+    def load_checkpoint(self, path):
+        """Resume a checkpoint file; returns the bound count it stored."""
+        v = ctypes.c_uint64(0)
+        _check(lib().pbb_load_checkpoint(self._h, os.fsencode(path), ctypes.byref(v)))
+        return v.value
 
     def set_wait_limit(self, seconds):
         """Longest host wait for one window (< 0: window + 60 s, 0: none);
@@ -359,6 +378,21 @@ def bound_children(p, sched, limit1, limit2, johnson_mode=0, device=0, method=No
     return out
 
 
+def fact_to_decimal(digits):
+    """Factoradic vector (digit i in [0, n-i)) -> decimal index string."""
+    d = np.ascontiguousarray(digits, dtype=np.int32)
+    buf = ctypes.create_string_buffer(128)
+    _check(lib().pbb_fact_to_decimal(len(d), _ptr(d), buf, 128))
+    return buf.value.decode()
+
+
+def decimal_to_fact(n, decimal):
+    """Decimal index (below n!) -> factoradic vector of n digits."""
+    d = np.zeros(n, np.int32)
+    _check(lib().pbb_decimal_to_fact(int(n), str(decimal).encode(), _ptr(d)))
+    return d
+
+
 def int32_peak(device=0):
     """Measured INT32 add+max throughput of the GPU in Gop/s."""
     g = ctypes.c_double(0.0)
@@ -374,6 +408,30 @@ def neh(p):
     cost = np.zeros(1, np.int32)
     _check(lib().pbb_neh(ctypes.byref(inst), _ptr(perm), _ptr(cost)))
     return int(cost[0]), perm
+
+
+def neh_batch(instances, device=0):
+    """NEH of many instances on the device (one warp each): list of
+    (cost, permutation), equal to neh() for each."""
+    cnt = len(instances)
+    keep = [np.ascontiguousarray(p, dtype=np.int32) for p in instances]
+    arr = (_Instance * cnt)(*[_Instance(p.shape[1], p.shape[0], _ptr(p)) for p in keep])
+    perms = np.zeros((cnt, MAX_JOBS), np.int32)
+    costs = np.zeros(cnt, np.int32)
+    _check(lib().pbb_neh_batch(arr, cnt, int(device), _ptr(perms), _ptr(costs)))
+    return [(int(costs[i]), perms[i, :keep[i].shape[1]].copy()) for i in range(cnt)]
+
+
+def ig_batch(instances, iterations=100, seed=0, device=0):
+    """Seeded iterated greedy from NEH on the device (one warp per instance):
+    list of (cost, permutation); instance i draws from seed + i."""
+    cnt = len(instances)
+    keep = [np.ascontiguousarray(p, dtype=np.int32) for p in instances]
+    arr = (_Instance * cnt)(*[_Instance(p.shape[1], p.shape[0], _ptr(p)) for p in keep])
+    perms = np.zeros((cnt, MAX_JOBS), np.int32)
+    costs = np.zeros(cnt, np.int32)
+    _check(lib().pbb_ig_batch(arr, cnt, int(device), int(iterations), int(seed), _ptr(perms), _ptr(costs)))
+    return [(int(costs[i]), perms[i, :keep[i].shape[1]].copy()) for i in range(cnt)]
 
 
 class PoolConfig:

@@ -16,8 +16,10 @@ CLI = os.path.join(PKG, "bb")
 ARCH = ["-gencode", "arch=compute_100a,code=sm_100a"]
 NVFLAGS = ARCH + ["-lineinfo", "-O3", "-std=c++17", "-Xcompiler", "-fPIC"]
 
-LIB_SOURCES = ["pbb_kernels.cu", "pbb_host.cu", "pbb_diag.cu", "pbb_noalloc.cu", "pbb_pool.cu"]
-LIB_DEPS = LIB_SOURCES + ["pbb_types.h", "pbb_device.cuh", "pbb_launch.h", "pbb_tables.h"]
+LIB_SOURCES = ["pbb_kernels.cu", "pbb_host.cu", "pbb_diag.cu", "pbb_noalloc.cu", "pbb_pool.cu", "pbb_heur.cu",
+               "pbb_ckpt.cu"]
+LIB_DEPS = LIB_SOURCES + ["pbb_types.h", "pbb_device.cuh", "pbb_launch.h", "pbb_tables.h", "pbb_heur.h",
+                          "pbb_devguard.h"]
 HEADERS = ["pbbperm.h", "pbbperm_diag.h"]
 
 

@@ -15,6 +15,7 @@
 #include "pbb_devguard.h"
 #include "pbb_launch.h"
 #include "pbb_tables.h"
+#include "pbb_heur.h"
 #include "../../include/pbbperm.h"
 #include "../../include/pbbperm_diag.h"
 
@@ -103,6 +104,15 @@ namespace pbbh {
 void set_error(const char* msg) { g_err = msg; }
 }  // namespace pbbh
 
+struct pbb_engine;
+namespace pbbh {
+// engine facts for the checkpoint code (pbb_ckpt.cu)
+int engine_jobs(const pbb_engine* e);
+int engine_explorers(const pbb_engine* e);
+const std::vector<int32_t>& engine_root(const pbb_engine* e);
+void engine_set_start_perm(pbb_engine* e, const int32_t* perm);
+}  // namespace pbbh
+
 // ---------------------------------------------------------------------------
 // engine
 // ---------------------------------------------------------------------------
@@ -129,12 +139,24 @@ struct pbb_engine {
     double slice_s = 2.0;
     int select_budget = 4096;
     int max_rounds = INT_MAX;      // explorer loop rounds per launch
+    int* neh_d = nullptr;          // device NEH result: perm[64], cost
+    NehTask* neh_task_d = nullptr; // the engine's instance as a heuristic task
+    bool from_neh = false;         // the current search started from PBB_UB_NEH
+    std::vector<int32_t> root;     // root permutation of the current search
+    std::vector<int32_t> start_perm;   // schedule of the starting bound (e.g. a checkpoint's incumbent)
     SampleBuf* sample_d = nullptr; // node sampling (diagnostic), NULL when off
     int* sample_rec = nullptr;
     int sample_stride = 0;
     double wait_limit_s = -1.0;    // host wait per window: < 0 window + 60 s, 0 unbounded
     bool pending = false;          // a window whose wait ran out is still on the stream
 };
+
+namespace pbbh {
+int engine_jobs(const pbb_engine* e) { return e->H.n; }
+int engine_explorers(const pbb_engine* e) { return e->cfg.nb_ivms; }
+const std::vector<int32_t>& engine_root(const pbb_engine* e) { return e->root; }
+void engine_set_start_perm(pbb_engine* e, const int32_t* perm) { e->start_perm.assign(perm, perm + e->H.n); }
+}  // namespace pbbh
 
 namespace {
 
@@ -259,6 +281,8 @@ int pbb_engine_destroy(pbb_engine* e)
     cudaFree(e->ngroups_d);
     cudaFree(e->sample_d);
     cudaFree(e->sample_rec);
+    cudaFree(e->neh_d);
+    cudaFree(e->neh_task_d);
     if (e->ev0) cudaEventDestroy(e->ev0);
     if (e->ev1) cudaEventDestroy(e->ev1);
     if (e->st) cudaStreamDestroy(e->st);
@@ -302,6 +326,18 @@ static int engine_create(const pbb_instance* inst, const pbb_config* cfg, pbb_en
     CK(cudaMalloc(&e->qseq, sizeof(unsigned) * B));
     CK(cudaMalloc(&e->ub_d, sizeof(int)));
     CK(cudaMalloc(&e->root_d, sizeof(int) * PBB_MAX_N));
+    CK(cudaMalloc(&e->neh_d, sizeof(int) * (PBB_MAX_N + 1)));
+    CK(cudaMalloc(&e->neh_task_d, sizeof(NehTask)));
+    {
+        NehTask t;
+        t.p = e->di.p;
+        t.n = H.n;
+        t.m = H.m;
+        t.perm = e->neh_d;
+        t.cost = e->neh_d + PBB_MAX_N;
+        t.ub = e->ub_d;
+        CK(cudaMemcpyAsync(e->neh_task_d, &t, sizeof(t), cudaMemcpyHostToDevice, e->st));
+    }
     CK(cudaMalloc(&e->ival_d, sizeof(int) * 2 * PBB_MAX_N));
     CK(cudaMalloc(&e->ctl, sizeof(GroupCtl)));
     CK(cudaMalloc(&e->group_d, sizeof(DevGroup)));
@@ -382,14 +418,20 @@ static int start_impl(pbb_engine* e, int32_t ub, const int32_t* root_perm, const
         iv[i] = p;
         iv[PBB_MAX_N + i] = q;
     }
-    if (ub < 0) return fail(PBB_E_INVAL, "ub must be >= 0");
+    if (ub < 0 && ub != PBB_UB_NEH) return fail(PBB_E_INVAL, "ub must be >= 0 (or PBB_UB_NEH)");
     e->ub = ub;
+    e->from_neh = ub == PBB_UB_NEH;
+    e->root.assign(root.begin(), root.begin() + n);
+    e->start_perm.clear();
     CK(cudaMemcpyAsync(e->ub_d, &ub, sizeof(int), cudaMemcpyHostToDevice, e->st));
+    // the device NEH writes its makespan where the reset kernel reads the bound
+    if (e->from_neh) CK(pbbl::launch_neh(e->neh_task_d, 1, e->st));
     CK(cudaMemcpyAsync(e->root_d, root.data(), sizeof(int) * PBB_MAX_N, cudaMemcpyHostToDevice, e->st));
     CK(cudaMemcpyAsync(e->ival_d, iv.data(), sizeof(int) * 2 * PBB_MAX_N, cudaMemcpyHostToDevice, e->st));
     CK(pbbl::launch_reset(e->group_d, 1, e->ub_d, e->st));
     CK(pbbl::launch_root(e->nw, e->group_d, 1, e->root_d, e->ival_d, PBB_MAX_N, e->root_smem, e->st));
     CK(cudaStreamSynchronize(e->st));
+    if (e->from_neh) CK(cudaMemcpy(&e->ub, e->ub_d, sizeof(int), cudaMemcpyDeviceToHost));
     e->pending = false;
     GroupCtl c;
     CK(cudaMemcpy(&c, e->ctl, sizeof(c), cudaMemcpyDeviceToHost));
@@ -414,7 +456,7 @@ int pbb_init_from_fac(pbb_engine* e, int32_t ub, const int32_t* root_perm, int32
     if (!pos || !end) return fail(PBB_E_INVAL, "pos/end are NULL");
     const int B = e->cfg.nb_ivms;
     if (nb_intervals < 1 || nb_intervals > B) return fail(PBB_E_INVAL, "nb_intervals must be in [1, nb_ivms]");
-    if (ub < 0) return fail(PBB_E_INVAL, "ub must be >= 0");
+    if (ub < 0 && ub != PBB_UB_NEH) return fail(PBB_E_INVAL, "ub must be >= 0 (or PBB_UB_NEH)");
     pbbh::DeviceGuard keep_callers_device;
     CK(cudaSetDevice(e->dev));
     const int n = e->H.n;
@@ -448,6 +490,7 @@ int pbb_init_from_fac(pbb_engine* e, int32_t ub, const int32_t* root_perm, int32
     if (!err) err = cudaMemcpyAsync(ival_d, iv.data(), sizeof(int) * iv.size(), cudaMemcpyHostToDevice, e->st);
     if (!err) err = cudaMemcpyAsync(ids_d, id.data(), sizeof(int) * nb_intervals, cudaMemcpyHostToDevice, e->st);
     if (!err) err = cudaMemcpyAsync(e->ub_d, &ub, sizeof(int), cudaMemcpyHostToDevice, e->st);
+    if (!err && ub == PBB_UB_NEH) err = pbbl::launch_neh(e->neh_task_d, 1, e->st);
     if (!err) err = cudaMemcpyAsync(e->root_d, root.data(), sizeof(int) * PBB_MAX_N, cudaMemcpyHostToDevice, e->st);
     if (!err) err = pbbl::launch_reset(e->group_d, 1, e->ub_d, e->st);
     if (!err)
@@ -461,6 +504,10 @@ int pbb_init_from_fac(pbb_engine* e, int32_t ub, const int32_t* root_perm, int32
     GroupCtl c;
     CK(cudaMemcpy(&c, e->ctl, sizeof(c), cudaMemcpyDeviceToHost));
     e->ub = ub;
+    e->from_neh = ub == PBB_UB_NEH;
+    if (e->from_neh) CK(cudaMemcpy(&e->ub, e->ub_d, sizeof(int), cudaMemcpyDeviceToHost));
+    e->root.assign(root.begin(), root.begin() + n);
+    e->start_perm.clear();
     e->started = true;
     e->done = (c.active == 0);
     e->dev_seconds = 0.0;
@@ -678,6 +725,17 @@ int pbb_get_result(pbb_engine* e, pbb_result* out)
         signed char buf[PBB_MAX_N];
         CK(cudaMemcpy(buf, e->bestperm + (size_t)id * PBB_MAX_N, PBB_MAX_N, cudaMemcpyDeviceToHost));
         for (int i = 0; i < e->H.n; i++) out->perm[i] = buf[i];
+        out->has_perm = 1;
+    } else if (e->from_neh && out->cost == e->ub) {
+        // not improved: the NEH schedule the search started from
+        int buf[PBB_MAX_N + 1];
+        CK(cudaMemcpy(buf, e->neh_d, sizeof(buf), cudaMemcpyDeviceToHost));
+        for (int i = 0; i < e->H.n; i++) out->perm[i] = buf[i];
+        out->has_perm = 1;
+    } else if ((int)e->start_perm.size() == e->H.n && out->cost == e->ub) {
+        // not improved: the schedule that came with the starting bound
+        for (int i = 0; i < e->H.n; i++) out->perm[i] = e->start_perm[i];
+        out->has_perm = 1;
     }
     return PBB_OK;
 }

@@ -19,6 +19,7 @@
 #include "pbb_devguard.h"
 #include "pbb_launch.h"
 #include "pbb_tables.h"
+#include "pbb_heur.h"
 #include "../../include/pbbperm.h"
 
 namespace {
@@ -55,6 +56,7 @@ struct Slot {
     size_t off = 0, bytes = 0;      // explorer arena block
     int explorers = 0;
     int windows = 0;
+    bool from_neh = false;          // started from the device NEH bound
     DevGroup g{};
 };
 
@@ -116,6 +118,8 @@ struct pbb_pool {
     int* ub_d = nullptr;
     int* roots_d = nullptr;
     int* ivals_d = nullptr;
+    int* neh_d = nullptr;         // per slot: device NEH permutation [64] and makespan
+    NehTask* neh_tasks_d = nullptr;
     cudaGraphExec_t window = nullptr;
     std::vector<Slot> slots;
     // the FIFO and the finished results are shared with submitting and
@@ -125,6 +129,7 @@ struct pbb_pool {
     std::vector<pbb_pool_result> done;
     Arena alloc;
     std::vector<int> pending_ub, pending_root;   // of the instances admitted in this step
+    std::vector<NehTask> pending_neh;            // admitted instances that start from device NEH
 };
 
 extern "C" void pbb_pool_config_default(pbb_pool_config* c)
@@ -157,6 +162,8 @@ extern "C" int pbb_pool_destroy(pbb_pool* P)
     cudaFree(P->ub_d);
     cudaFree(P->roots_d);
     cudaFree(P->ivals_d);
+    cudaFree(P->neh_d);
+    cudaFree(P->neh_tasks_d);
     if (P->st) cudaStreamDestroy(P->st);
     delete P;
     return PBB_OK;
@@ -260,6 +267,8 @@ int pool_create(const pbb_pool_config* in, pbb_pool* P)
     PCK(cudaMalloc(&P->ub_d, sizeof(int) * S), "bounds");
     PCK(cudaMalloc(&P->roots_d, sizeof(int) * S * PBB_MAX_N), "roots");
     PCK(cudaMalloc(&P->ivals_d, sizeof(int) * S * 2 * PBB_MAX_N), "intervals");
+    PCK(cudaMalloc(&P->neh_d, sizeof(int) * S * (PBB_MAX_N + 1)), "heuristic results");
+    PCK(cudaMalloc(&P->neh_tasks_d, sizeof(NehTask) * S), "heuristic tasks");
     P->arena_bytes = (size_t)c.explorer_bytes;
     const int E = P->epw;
     if (explorer_block_bytes(E, P->npad) > P->arena_bytes)
@@ -309,7 +318,7 @@ extern "C" int pbb_pool_submit(pbb_pool* P, const pbb_instance* inst, const pbb_
     if (!inst || !inst->p) return pfail(PBB_E_INVAL, "instance is NULL");
     if (inst->n_jobs > P->cfg.max_jobs || inst->n_machines > P->cfg.max_machines)
         return pfail(PBB_E_INVAL, "instance larger than the pool's max_jobs x max_machines");
-    if (ub < 0) return pfail(PBB_E_INVAL, "ub must be >= 0");
+    if (ub < 0 && ub != PBB_UB_NEH) return pfail(PBB_E_INVAL, "ub must be >= 0 (or PBB_UB_NEH)");
     Request r;
     r.tag = tag;
     pbb_config_default(&r.search);
@@ -401,6 +410,19 @@ int admit(pbb_pool* P, std::vector<int>& admitted)
         g.ctl = P->ctl + s;
         admitted.push_back(s);
         P->pending_ub.push_back(r.ub);
+        sl.from_neh = r.ub == PBB_UB_NEH;
+        if (sl.from_neh) {
+            // device NEH at admission: its makespan lands in this admission's
+            // bound slot before the reset kernel reads it
+            NehTask t;
+            t.p = g.inst.p;
+            t.n = H.n;
+            t.m = H.m;
+            t.perm = P->neh_d + (size_t)s * (PBB_MAX_N + 1);
+            t.cost = t.perm + PBB_MAX_N;
+            t.ub = P->ub_d + (P->pending_ub.size() - 1);
+            P->pending_neh.push_back(t);
+        }
         P->pending_root.insert(P->pending_root.end(), r.root.begin(), r.root.end());
     }
     return PBB_OK;
@@ -416,6 +438,7 @@ extern "C" int pbb_pool_step(pbb_pool* P, int32_t* resident, int32_t* queued)
     std::vector<int> admitted;
     P->pending_ub.clear();
     P->pending_root.clear();
+    P->pending_neh.clear();
     int rc = admit(P, admitted);
     if (rc) return rc;
     const int na = (int)admitted.size();
@@ -438,6 +461,12 @@ extern "C" int pbb_pool_step(pbb_pool* P, int32_t* resident, int32_t* queued)
                             cudaMemcpyHostToDevice, P->st), "upload");
         PCK(cudaMemcpyAsync(P->ivals_d, iv.data(), sizeof(int) * iv.size(), cudaMemcpyHostToDevice, P->st),
             "upload");
+        if (!P->pending_neh.empty()) {
+            const int nn = (int)P->pending_neh.size();
+            PCK(cudaMemcpyAsync(P->neh_tasks_d, P->pending_neh.data(), sizeof(NehTask) * nn, cudaMemcpyHostToDevice,
+                                P->st), "upload");
+            PCK(pbbl::launch_neh(P->neh_tasks_d, nn, P->st), "heuristic launch");
+        }
         PCK(pbbl::launch_reset(P->new_d, na, P->ub_d, P->st), "reset launch");
         PCK(pbbl::launch_root(P->nw, P->new_d, na, P->roots_d, P->ivals_d, PBB_MAX_N, P->root_smem, P->st),
             "root launch");
@@ -502,6 +531,14 @@ extern "C" int pbb_pool_step(pbb_pool* P, int32_t* resident, int32_t* queued)
             PCK(cudaMemcpy(buf, sl.g.ivm.bestperm + (size_t)id * sl.g.ivm.npad, sl.n, cudaMemcpyDeviceToHost),
                 "result read-back");
             for (int j = 0; j < sl.n; j++) r.perm[j] = buf[j];
+            r.has_perm = 1;
+        } else if (ok && sl.from_neh) {
+            // not improved: the device NEH schedule is optimal
+            int buf[PBB_MAX_N + 1];
+            PCK(cudaMemcpy(buf, P->neh_d + (size_t)s * (PBB_MAX_N + 1), sizeof(buf), cudaMemcpyDeviceToHost),
+                "result read-back");
+            for (int j = 0; j < sl.n; j++) r.perm[j] = buf[j];
+            r.has_perm = buf[PBB_MAX_N] == r.cost ? 1 : 0;
         }
         {
             std::lock_guard<std::mutex> lock(P->mu);
