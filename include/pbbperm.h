@@ -82,6 +82,9 @@ typedef struct pbb_config {
                                    (ivm_bound.cpp:506-544): 1 the chosen side's bound, 2 that bound
                                    minus the other side's, 3 the weak bound's idle time (not with
                                    boundingMode 1); 4 is rejected */
+    int32_t core_warps;         /* work sharing: warps per CTA that ask for work whatever the search's
+                                   width; the others join once it is wide (0 = 8) */
+    int32_t split_depth;        /* work sharing: no split at levels deeper than n - split_depth (0 = 10) */
 } pbb_config;
 
 typedef struct pbb_stats {
@@ -197,10 +200,15 @@ typedef struct pbb_pool_config {
     int32_t warps_per_cta;       /* block shape: warps per CTA (0 = 8) */
     int32_t ctas_per_instance;   /* cap on the CTAs one instance gets in a window (0 = none); every
                                     window spreads all resident CTAs evenly over the instances */
-    int32_t explorers_per_instance; /* explorers (IVMs) of each instance (0 = one per warp of the grid) */
-    int32_t pad;
+    int32_t explorers_per_instance; /* explorers (IVMs) of each instance (0 = one per warp of the widest
+                                       grid) */
+    int32_t tail_warps;          /* block shape of the tail: once nothing waits and few instances remain,
+                                    windows run CTAs of this many warps (0 = 20; < 0 or <= warps_per_cta:
+                                    no tail shape) */
     double window_s;             /* device time of one window (0 = 0.005) */
     int64_t explorer_bytes;      /* explorer memory budget (0 = 8 GiB) */
+    int32_t core_warps;          /* work sharing of every instance, as pbb_config (0 = 8) */
+    int32_t split_depth;         /* as pbb_config (0 = 10) */
 } pbb_pool_config;
 
 typedef struct pbb_pool_result {

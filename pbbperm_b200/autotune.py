@@ -1,39 +1,67 @@
 """Autotuner of the resident pool's shape for a batch of instances.
 
-Times pbb_batch_solve on a calibration sample (every k-th instance of the
-batch, same bounds) for each candidate block shape (warps per CTA) and explorers
-per instance, and returns the fastest PoolConfig with the
-timings of all candidates.
+Times pbb_batch_solve on a calibration sample of the batch and searches, one
+dimension at a time from the defaults (coordinate descent, each dimension's
+best value kept before the next is tried):
+
+  warps_per_cta           block shape of the bulk of the batch
+  tail_warps              block shape once few instances remain (0 = 20 warps, -1 = none)
+  core_warps              warps per CTA that always ask for work (steal threshold)
+  split_depth             no split deeper than n - split_depth (steal threshold)
+  explorers_per_instance  explorers of each resident instance (0 = one per warp of the widest grid)
+
+The sample is every k-th instance plus the largest ones (jobs x machines):
+a batch ends with its heaviest searches, which a uniform sample misses.
+Returns the fastest PoolConfig and the timings of every trial.
 """
-import itertools
 import time
 
 import pbbperm_b200 as pb
 
-CANDIDATES = {
-    "warps_per_cta": (4, 8, 16),
-    # 0: one explorer per warp of the grid, so that an instance left alone at
-    # the end of a batch can still use the whole GPU (a calibration sample
-    # does not show that tail)
-    "explorers_per_instance": (0,),
-}
+CANDIDATES = [
+    ("warps_per_cta", (8, 4, 16)),
+    ("tail_warps", (0, -1)),
+    ("core_warps", (8, 4)),
+    ("split_depth", (10, 6, 14)),
+    ("explorers_per_instance", (0, 1024)),
+]
 
 
-def tune_pool(instances, ubs, search, max_jobs, max_machines, sample=48, window_s=0.01, device=0, repeats=1):
-    step = max(1, len(instances) // sample)
-    cal = instances[::step][:sample]
-    cal_ub = ubs[::step][:sample]
+def calibration_sample(instances, ubs, size=32, largest=2):
+    order = sorted(range(len(instances)), key=lambda i: (-instances[i].size, -instances[i].shape[1], i))
+    top = order[:largest]
+    step = max(1, len(instances) // size)
+    idx = sorted(set(top) | set(range(0, len(instances), step)))
+    return [instances[i] for i in idx], [ubs[i] for i in idx]
+
+
+def tune_pool(instances, ubs, search, max_jobs, max_machines, sample=32, window_s=0.01, device=0, repeats=1,
+              largest=2):
+    cal, cal_ub = calibration_sample(instances, ubs, sample, largest)
+    current = {k: v[0] for k, v in CANDIDATES}
     trials = []
-    best = None
-    for w, e in itertools.product(CANDIDATES["warps_per_cta"], CANDIDATES["explorers_per_instance"]):
-        pc = pb.PoolConfig(max_jobs=max_jobs, max_machines=max_machines, warps_per_cta=w, explorers_per_instance=e,
-                           window_s=window_s, device=device)
+    cache = {}
+
+    def timed(cfg):
+        key = tuple(sorted(cfg.items()))
+        if key in cache:
+            return cache[key]
+        pc = pb.PoolConfig(max_jobs=max_jobs, max_machines=max_machines, window_s=window_s, device=device, **cfg)
         t = float("inf")
         for _ in range(repeats):
             t0 = time.perf_counter()
             pb.batch_solve(cal, ubs=cal_ub, config=search, pool_config=pc)
             t = min(t, time.perf_counter() - t0)
-        trials.append(dict(warps_per_cta=w, explorers_per_instance=e, seconds=round(t, 4)))
-        if best is None or t < best[0]:
-            best = (t, pc)
-    return best[1], trials
+        cache[key] = t
+        trials.append(dict(cfg, seconds=round(t, 4)))
+        return t
+
+    best_t = timed(current)
+    for name, values in CANDIDATES:
+        for v in values[1:]:
+            trial = dict(current, **{name: v})
+            t = timed(trial)
+            if t < best_t:
+                best_t, current = t, trial
+    pc = pb.PoolConfig(max_jobs=max_jobs, max_machines=max_machines, window_s=window_s, device=device, **current)
+    return pc, trials

@@ -354,6 +354,8 @@ static int engine_create(const pbb_instance* inst, const pbb_config* cfg, pbb_en
     g.search.find_all = cfg->find_all ? 1 : 0;
     g.search.sort_nodes = cfg->sorted_dfs;
     g.search.sort_crit = cfg->sorting_criterion;
+    g.search.core_warps = cfg->core_warps > 0 ? cfg->core_warps : PBB_CORE_WARPS;
+    g.search.split_depth = cfg->split_depth > 0 ? cfg->split_depth : PBB_SPLIT_DEPTH;
     g.search.early_stop = cfg->early_stop_johnson ? 1 : 0;
     g.ivm.count = B;
     g.ivm.npad = npad;

@@ -458,7 +458,7 @@ __device__ __forceinline__ int try_share(const DevGroup& G, int id, Ivm<NW>& R)
         const unsigned d = __ballot_sync(FULLMASK, lv < n && R.pos[w] != R.end[w]);
         if (d) f = w * 32 + __ffs(d) - 1;
     }
-    const int lcap = n - 10 > 0 ? n - 10 : 0;
+    const int lcap = max(n - G.search.split_depth, 0);
     int l = f;
     if (l > R.line) l = R.line;
     if (l > lcap) l = lcap;
@@ -736,10 +736,11 @@ pbb_explore_kernel(const DevGroup* groups, const int* ngroups_d, int warps_per_c
     WarpCounters C = {0, 0, 0, 0, 0, 0, 0, 0, 0};
     Ivm<NW> R;
     int cached = -1;                   // explorer whose state is held in registers
-    // explorers holding work once the first PBB_CORE_WARPS warps of every CTA
+    // explorers holding work once the first core_warps warps of every CTA
     // are busy (no more than that share of the explorers can be)
-    const int core_active = min(PBB_CORE_WARPS * G.ctas,
-                                (int)((long long)G.ivm.count * PBB_CORE_WARPS / warps_per_cta));
+    const int core_warps = G.search.core_warps;
+    const int core_active = min(core_warps * G.ctas, (int)((long long)G.ivm.count * core_warps / warps_per_cta));
+    const bool core_warp = wic < core_warps;   // this warp always asks for work
     unsigned idle_ns = 500;            // back-off of a warp that found nothing to do
     int best = 0;
     if (lane_id() == 0) best = (int)(ld_volatile_u64(&G.ctl->best_key) >> 32);
@@ -810,11 +811,11 @@ pbb_explore_kernel(const DevGroup* groups, const int* ngroups_d, int warps_per_c
         // A warp with nothing to do offers ONE of its idle explorers to the
         // donors: work is only split towards warps that would otherwise wait,
         // never towards a warp that is busy with another explorer.  The first
-        // PBB_CORE_WARPS warps of every CTA always take part; the others join
+        // core_warps warps of every CTA always take part; the others join
         // once that many explorers per CTA hold work, so a narrow search is
         // not cut into pieces for warps it cannot feed, and a wide one still
         // gets every warp.
-        const bool tier = wic < PBB_CORE_WARPS || active >= core_active;
+        const bool tier = core_warp || active >= core_active;
         if (!busy && spare >= 0 && lane_id() == 0 && tier) {
             st_release(G.ivm.state + spare, IVM_QUEUED);
             if (!queue_push(G, spare)) st_release(G.ivm.state + spare, IVM_IDLE);

@@ -103,7 +103,9 @@ struct pbb_pool {
     cudaStream_t st = nullptr;
     int nw = 1, npad = 32, warps = 8, cpi = 1, epw = 1, smem = 0, root_smem = 0;
     int max_slots = 0;          // resident instances at most
-    int grid = 0;               // CTAs of every window launch (max_slots x cpi)
+    int grid = 0;               // CTAs of a window launch (all the CTAs of this shape the GPU holds)
+    int tail_warps = 0, tail_grid = 0, tail_smem = 0;   // the tail's block shape (0 warps: none)
+    int core_warps = PBB_CORE_WARPS, split_depth = PBB_SPLIT_DEPTH;
     int Ppad_max = 0;
     size_t table_stride = 0;
     size_t off_je = 0, off_p = 0, off_pm = 0, off_mt = 0, off_posj = 0;
@@ -121,6 +123,7 @@ struct pbb_pool {
     int* neh_d = nullptr;         // per slot: device NEH permutation [64] and makespan
     NehTask* neh_tasks_d = nullptr;
     cudaGraphExec_t window = nullptr;
+    cudaGraphExec_t window_tail = nullptr;   // the same window with the tail's block shape
     std::vector<Slot> slots;
     // the FIFO and the finished results are shared with submitting and
     // polling threads; everything else belongs to the thread driving step()
@@ -152,6 +155,7 @@ extern "C" int pbb_pool_destroy(pbb_pool* P)
     cudaSetDevice(P->dev);
     if (P->st) cudaStreamSynchronize(P->st);
     if (P->window) cudaGraphExecDestroy(P->window);
+    if (P->window_tail) cudaGraphExecDestroy(P->window_tail);
     cudaFree(P->arena);
     cudaFree(P->tables);
     cudaFree(P->ctl);
@@ -228,6 +232,8 @@ int pool_create(const pbb_pool_config* in, pbb_pool* P)
     P->warps = c.warps_per_cta;
     P->cpi = c.ctas_per_instance;
     P->epw = c.explorers_per_instance;
+    P->core_warps = c.core_warps > 0 ? c.core_warps : PBB_CORE_WARPS;
+    P->split_depth = c.split_depth > 0 ? c.split_depth : PBB_SPLIT_DEPTH;
     const int Pmax = c.max_machines * (c.max_machines - 1) / 2;
     P->Ppad_max = (Pmax + 31) / 32 * 32;
     P->smem = pbbl::smem_bytes(c.max_jobs, c.max_machines, P->Ppad_max, P->warps);
@@ -243,9 +249,21 @@ int pool_create(const pbb_pool_config* in, pbb_pool* P)
     int capacity = sms * per_sm;
     if (capacity < 1) capacity = 1;
     P->grid = capacity;
-    // default explorer count: every warp of the grid owns one, so that an
-    // instance left alone at the end of a batch can keep the whole GPU busy
-    if (P->epw <= 0) P->epw = P->grid * P->warps;
+    // the tail's block shape: wider CTAs once few instances remain (the heavy
+    // searches that finish last want every warp an SM holds)
+    const int tw = c.tail_warps == 0 ? PBB_WARPS_MAX : c.tail_warps;
+    if (tw > P->warps && tw <= PBB_WARPS_MAX) {
+        const int ts = pbbl::smem_bytes(c.max_jobs, c.max_machines, P->Ppad_max, tw);
+        const int tper = ts <= optin ? pbbl::explore_ctas_per_sm(P->nw, tw, ts) : 0;
+        if (tper >= 1) {
+            P->tail_warps = tw;
+            P->tail_smem = ts;
+            P->tail_grid = sms * tper;
+        }
+    }
+    // default explorer count: every warp of the widest grid owns one, so that
+    // an instance left alone at the end of a batch can keep the whole GPU busy
+    if (P->epw <= 0) P->epw = std::max(P->grid * P->warps, P->tail_grid * P->tail_warps);
     P->max_slots = c.max_resident > 0 ? std::min(c.max_resident, capacity) : capacity;
     // per-slot instance tables
     P->off_je = 0;
@@ -292,6 +310,21 @@ int pool_create(const pbb_pool_config* in, pbb_pool* P)
     cudaError_t e5 = cudaGraphInstantiate(&P->window, graph, 0);
     cudaGraphDestroy(graph);
     if (e5) return pfail(PBB_E_CUDA, "instantiating the window graph failed");
+    if (P->tail_warps > 0) {
+        graph = nullptr;
+        PCK(cudaStreamBeginCapture(P->st, cudaStreamCaptureModeRelaxed), "graph capture");
+        e1 = pbbl::launch_explore(P->nw, P->groups_d, P->ngroups_d, P->tail_grid, P->tail_warps, P->tail_smem,
+                                  budget, INT_MAX, 4096, P->st);
+        e3 = cudaMemcpyAsync(P->ctl_h, P->ctl, sizeof(GroupCtl) * S, cudaMemcpyDeviceToHost, P->st);
+        e4 = cudaStreamEndCapture(P->st, &graph);
+        if (e1 || e3 || e4) {
+            if (graph) cudaGraphDestroy(graph);
+            return pfail(PBB_E_CUDA, "capturing the tail window graph failed");
+        }
+        e5 = cudaGraphInstantiate(&P->window_tail, graph, 0);
+        cudaGraphDestroy(graph);
+        if (e5) return pfail(PBB_E_CUDA, "instantiating the tail window graph failed");
+    }
     return PBB_OK;
 }
 
@@ -406,6 +439,8 @@ int admit(pbb_pool* P, std::vector<int>& admitted)
         // the pool's window graph runs the default explorer, which has no early
         // Johnson exit: it leaves every decision unchanged, so it is not needed
         g.search.early_stop = 0;
+        g.search.core_warps = P->core_warps;
+        g.search.split_depth = P->split_depth;
         carve_explorers(P->arena + off, E, P->npad, g.ivm);
         g.ctl = P->ctl + s;
         admitted.push_back(s);
@@ -479,13 +514,22 @@ extern "C" int pbb_pool_step(pbb_pool* P, int32_t* resident, int32_t* queued)
         act.push_back(P->slots[s].g);
         act_slot.push_back(s);
     }
+    // the tail: nothing waits and few instances remain -- wide CTAs, at least
+    // four per resident instance
+    bool waiting;
+    {
+        std::lock_guard<std::mutex> lock(P->mu);
+        waiting = !P->queue.empty();
+    }
+    const bool tail = P->tail_warps > 0 && !waiting && (int)act.size() * 4 <= P->tail_grid;
+    const int grid = tail ? P->tail_grid : P->grid;
     {
         // all resident CTAs, spread evenly (a lone instance in the tail of a
         // batch gets the whole GPU), capped by ctas_per_instance when set
         const int na = (int)act.size();
         int first = 0;
         for (int i = 0; i < na; i++) {
-            int c = P->grid / std::max(1, na) + (i < P->grid % std::max(1, na) ? 1 : 0);
+            int c = grid / std::max(1, na) + (i < grid % std::max(1, na) ? 1 : 0);
             if (P->cpi > 0 && c > P->cpi) c = P->cpi;
             if (c < 1) c = 1;
             act[i].first_cta = first;
@@ -499,7 +543,7 @@ extern "C" int pbb_pool_step(pbb_pool* P, int32_t* resident, int32_t* queued)
             "upload");
     }
     PCK(cudaMemcpyAsync(P->ngroups_d, &nact, sizeof(int), cudaMemcpyHostToDevice, P->st), "upload");
-    if (nact > 0) PCK(cudaGraphLaunch(P->window, P->st), "window launch");
+    if (nact > 0) PCK(cudaGraphLaunch(tail ? P->window_tail : P->window, P->st), "window launch");
     PCK(cudaStreamSynchronize(P->st), "window");
     // retire the finished instances
     for (int i = 0; i < nact; i++) {

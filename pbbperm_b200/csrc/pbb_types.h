@@ -5,9 +5,8 @@
 #define PBB_MAX_N 64          // jobs per instance (int8 IVM cells, two 32-bit mask words)
 #define PBB_MAX_M 32          // machines per instance (one machine per lane in recurrences)
 #define PBB_WARPS_MAX 20      // explorer warps per CTA (96 registers a thread)
-#ifndef PBB_CORE_WARPS
-#define PBB_CORE_WARPS 8      // warps per CTA that ask for work whatever the search's width
-#endif
+#define PBB_CORE_WARPS 8      // default of DevSearch::core_warps
+#define PBB_SPLIT_DEPTH 10    // default of DevSearch::split_depth
 
 // IVM life cycle (per explorer, in global memory)
 #define IVM_IDLE 0            // no interval
@@ -51,6 +50,8 @@ struct DevSearch {
                        //      2 and 4 by (cost, priority), 3 by priority
     int sort_crit;     // [bb] sortingCriterion (sortedDFS >= 2): 1 cost, 2 cost minus the other side's, 3 idle time
     int early_stop;    // [bb] earlyStopJohnson: a child's Johnson scan may stop once it exceeds the incumbent
+    int core_warps;    // warps per CTA that ask for work whatever the search's width (1..warps per CTA)
+    int split_depth;   // work is not split at levels deeper than n - split_depth
 };
 
 // Per-group control block (device memory).

@@ -2,10 +2,11 @@
 
 batch: the batched configuration -- `count` instances of uneven size
 (pbbperm_b200.instances.batch_instance, seeds 100, 101, ...), weak then Johnson
-bound, initial bound NEH + 1 (so every instance returns an optimal
-permutation), all solved to optimality through one resident pool, against
-solving the same instances one at a time with the single-instance engine on
-the same GPU.
+bound, initial bound NEH computed on the device (PBB_UB_NEH: inside the timed
+solve, on both sides), all solved to optimality through one resident pool,
+against solving the same instances one at a time with the single-instance
+engine on the same GPU.  Every result carries an optimal schedule (a leaf's,
+or NEH's when nothing improves on it), re-verified here.
 
 serve: a Poisson request stream (instances.serving_instance, arrivals from
 instances.poisson_arrivals) served by the pool with continuous batching
@@ -36,19 +37,24 @@ def makespan(p, perm):
 SEARCH = pb.Config(boundingMode=2, adaptiveBranchingMode=3)
 
 
-def solo_solve(p, ub, nb_ivms=16384, device=0):
+def verified(p, r):
+    """The result holds a schedule whose makespan is its cost."""
+    return bool(r["has_perm"]) and makespan(p, r["perm"]) == r["cost"]
+
+
+def solo_solve(p, ub=pb.UB_NEH, nb_ivms=16384, device=0):
     with pb.Engine(p, pb.Config(boundingMode=2, adaptiveBranchingMode=3, nbIVMs=nb_ivms, device=device)) as e:
         return e.solve(ub=ub)
 
 
 def run_batch(count=512, pool_config=None, solo_sample=None, device=0):
     insts = [batch_instance(100 + i) for i in range(count)]
-    ubs = [pb.neh(p)[0] + 1 for p in insts]
+    ubs = [pb.UB_NEH] * count
     pc = pool_config or pb.PoolConfig(max_jobs=20, max_machines=20, window_s=0.02, device=device)
     t0 = time.perf_counter()
     res = pb.batch_solve(insts, ubs=ubs, config=SEARCH, pool_config=pc)
     t_batch = time.perf_counter() - t0
-    ok = all(r["found"] and makespan(p, r["perm"]) == r["cost"] for p, r in zip(insts, res))
+    ok = all(verified(p, r) for p, r in zip(insts, res))
     idx = list(range(count)) if not solo_sample else list(range(0, count, max(1, count // solo_sample)))
     t0 = time.perf_counter()
     solo = {i: solo_solve(insts[i], ubs[i], device=device) for i in idx}
@@ -58,18 +64,21 @@ def run_batch(count=512, pool_config=None, solo_sample=None, device=0):
                 solo_instances=len(idx), solo_seconds=t_solo, solo_inst_per_s=len(idx) / t_solo,
                 speedup=(count / t_batch) / (len(idx) / t_solo), all_verified=ok, same_optima_as_solo=same,
                 nodes=int(sum(r["decomposed"] for r in res)),
-                pool={k: getattr(pc, k) for k in ("warps_per_cta", "explorers_per_instance",
-                                                  "window_s")})
+                pool={k: getattr(pc, k) for k in ("warps_per_cta", "tail_warps", "core_warps", "split_depth",
+                                                  "explorers_per_instance", "window_s")})
 
 
-def serve_stream(rate, seconds, seed=7, pool_config=None, device=0, max_requests=20000):
-    """Serve min(rate x seconds, max_requests) requests (at least 20) of the
-    Poisson stream through one pool; latency = completion - arrival."""
-    count = max(20, min(max_requests, int(rate * seconds)))
+def serve_stream(rate, count, seed=7, pool_config=None, device=0, max_resident=0):
+    """Serve `count` requests of the Poisson stream at `rate` through one pool
+    (continuous batching: arrivals join between windows as slots free up);
+    latency = completion - arrival.  max_resident = 1 serves the same stream
+    one request at a time through the same pool (the one-at-a-time side)."""
     arr = poisson_arrivals(seed, rate, count)
     insts = [serving_instance(10000 + i) for i in range(count)]
-    ubs = [pb.neh(p)[0] + 1 for p in insts]
+    ubs = [pb.UB_NEH] * count
     pc = pool_config or pb.PoolConfig(max_jobs=22, max_machines=20, window_s=0.002, device=device)
+    if max_resident:
+        pc = pb.PoolConfig(**{**vars(pc), "max_resident": max_resident})
     lat = {}
     with pb.Pool(pc) as pool:
         start = time.perf_counter()
@@ -90,7 +99,7 @@ def serve_stream(rate, seconds, seed=7, pool_config=None, device=0, max_requests
                     time.sleep(min(wait, 0.01))
         span = time.perf_counter() - start - arr[0]
     lats = sorted(v[0] for v in lat.values())
-    ok = all(r["found"] and makespan(insts[t], r["perm"]) == r["cost"] for t, (_, r) in lat.items())
+    ok = all(verified(insts[t], r) for t, (_, r) in lat.items())
     return dict(rate=rate, requests=count, throughput=count / span, p50_ms=1e3 * lats[len(lats) // 2],
                 p99_ms=1e3 * lats[min(len(lats) - 1, int(0.99 * len(lats)))], all_verified=ok,
                 costs={t: r["cost"] for t, (_, r) in lat.items()})
@@ -102,7 +111,7 @@ def alone_service(count, device=0):
     request sequence does not depend on the rate, so one measurement serves
     every rate of a sweep."""
     insts = [serving_instance(10000 + i) for i in range(count)]
-    ubs = [pb.neh(p)[0] + 1 for p in insts]
+    ubs = [pb.UB_NEH] * count
     service, costs = [], {}
     for i in range(count):
         t0 = time.perf_counter()
