@@ -60,8 +60,14 @@ def parse():
                     help="serve: requests timed through the single-instance engine")
     ap.add_argument("--batch-solo", type=int, default=0, help="batch: instances solved one at a time (0: all)")
     ap.add_argument("--warps-per-cta", type=int, default=0, help="explorer warps per CTA (0: as many as fit)")
-    ap.add_argument("--pool-window", type=float, default=0.02, help="device time per pool window (batch)")
+    ap.add_argument("--pool-window", type=float, default=0.0,
+                    help="device time per pool window (batch; 0: the autotuner's choice)")
     ap.add_argument("--config2", type=int, default=1, help="add the 20x20 solve-to-completion sub-object (N=1)")
+    ap.add_argument("--summary-batch", type=int, default=128,
+                    help="add a compact batched sub-object over this many instances (0: none; N=1)")
+    ap.add_argument("--summary-serve", type=int, default=200,
+                    help="add a compact served sub-object over this many requests (0: none; N=1)")
+    ap.add_argument("--summary-rate", type=float, default=1000.0, help="request rate of the served sub-object")
     return ap.parse_args()
 
 
@@ -321,6 +327,10 @@ def run_ours(args):
         extra = {}
         if ws == 1 and args.config2:
             extra["config2"] = run_config2(local)
+        if ws == 1 and args.summary_batch > 0:
+            extra["batch"] = compact_batch(args.summary_batch, local)
+        if ws == 1 and args.summary_serve > 0:
+            extra["serve"] = compact_serve(args.summary_serve, args.summary_rate, local)
         out = {"metric": METRIC, "value": round(value, 1), "unit": "nodes/s", "n_gpus": ws, "steps": steps_done,
                "warmup": args.warmup, "ms_per_step": round(max_s / max(1, steps_done) * 1e3, 3),
                "higher_is_better": True, "scaling": "weak", "vs_baseline": None, "dtype": "int32",
@@ -375,6 +385,42 @@ def run_config2(device):
             "device_seconds_all": [round(r["device_seconds"], 4) for r in runs]}
 
 
+# the pool shape the autotuner picks on the batched workload (bench.py
+# --workload batch): 8-warp CTAs in the bulk, 20-warp CTAs for the tail
+SUMMARY_POOL = dict(max_jobs=22, max_machines=20, warps_per_cta=8, tail_warps=0, window_s=0.02)
+
+
+def compact_batch(count, device):
+    """Batched form, compact: the first `count` instances of the batched
+    workload through one pool against the same instances one at a time
+    (single-instance engine, 16384 explorers), both from device NEH."""
+    import pbbperm_b200 as pb
+    from pbbperm_b200 import workloads
+    r = workloads.run_batch(count, pool_config=pb.PoolConfig(device=device, **SUMMARY_POOL), device=device)
+    return {"workload": "first %d instances of the batched workload (n 12-20, m 5/10/20, seeds 100+)" % count,
+            "batch_inst_per_s": round(r["batch_inst_per_s"], 2), "one_at_a_time_inst_per_s":
+            round(r["solo_inst_per_s"], 2), "speedup": round(r["speedup"], 2),
+            "all_verified": r["all_verified"], "same_optima": r["same_optima_as_solo"], "pool": r["pool"]}
+
+
+def compact_serve(count, rate, device):
+    """Served form, compact: `count` requests of the Poisson stream at `rate`
+    through the pool (continuous batching) and through a one-slot pool,
+    latency = completion - arrival, NEH computed on the device per request."""
+    import pbbperm_b200 as pb
+    from pbbperm_b200 import workloads
+    pc = pb.PoolConfig(device=device, **dict(SUMMARY_POOL, window_s=0.002))
+    mix = workloads.serve_stream(rate, count, pool_config=pc, device=device)
+    one = workloads.serve_stream(rate, count, pool_config=pc, device=device, max_resident=1)
+    row = {"workload": "serve-poisson-n10-22-m5-20, %d requests at %g req/s" % (count, rate)}
+    for name, r in (("mix", mix), ("one_at_a_time", one)):
+        row[name] = {"throughput": round(r["throughput"], 2), "p50_ms": round(r["p50_ms"], 2),
+                     "p99_ms": round(r["p99_ms"], 2), "all_verified": r["all_verified"]}
+    row["speedup"] = round(mix["throughput"] / one["throughput"], 2)
+    row["same_results_alone_and_in_mix"] = all(one["costs"][i] == mix["costs"][i] for i in mix["costs"])
+    return row
+
+
 def run_reference(args):
     ws, rank, _ = dist_env()
     if rank != 0:
@@ -420,7 +466,8 @@ def run_batch_bench(args):
     t0 = time.perf_counter()
     pc, trials = autotune.tune_pool(insts, ubs, workloads.SEARCH, max_jobs=20, max_machines=20, repeats=1)
     t_tune = time.perf_counter() - t0
-    pc.window_s = args.pool_window
+    if args.pool_window > 0:
+        pc.window_s = args.pool_window
     r = workloads.run_batch(args.batch_count, pool_config=pc, solo_sample=args.batch_solo)
     out = {"metric": "batched solve throughput (instances/s)", "value": round(r["batch_inst_per_s"], 2),
            "unit": "instances/s", "n_gpus": 1, "higher_is_better": True,

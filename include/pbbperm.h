@@ -23,6 +23,7 @@
  *                       (gpubb.h:155,171,172; gpubb.cu:1190-1310)
  *   pbb_bound_children  bound_abstract::boundChildren + bornes_calculer
  *                       (bounds/include/bound_abstract.h:15-26) for a batch of nodes
+ *   pbb_bound_children_ex  the same with the idle-time priorities and couts[1]
  *   pbb_neh             fastNEH::runNEH initial upper bound (heuristic/src/fastNEH.cpp:230-243)
  *   pbb_neh_batch       the same on the device for many instances (fastNEH.cpp:100-243)
  *   pbb_ig_batch        IG::runIG iterated greedy on the device (heuristic/src/IG.cpp:341-416)
@@ -203,8 +204,8 @@ typedef struct pbb_pool_config {
     int32_t explorers_per_instance; /* explorers (IVMs) of each instance (0 = one per warp of the widest
                                        grid) */
     int32_t tail_warps;          /* block shape of the tail: once nothing waits and few instances remain,
-                                    windows run CTAs of this many warps (0 = 20; < 0 or <= warps_per_cta:
-                                    no tail shape) */
+                                    windows run CTAs of this many warps and last at least 20 ms (0 = 20;
+                                    < 0 or <= warps_per_cta: no tail shape) */
     double window_s;             /* device time of one window (0 = 0.005) */
     int64_t explorer_bytes;      /* explorer memory budget (0 = 8 GiB) */
     int32_t core_warps;          /* work sharing of every instance, as pbb_config (0 = 8) */
@@ -249,6 +250,24 @@ int pbb_bound_children(const pbb_instance* inst, int32_t johnson_mode, int32_t d
                        const int32_t* sched, const int32_t* limit1, const int32_t* limit2,
                        int32_t* weak_begin, int32_t* weak_end, int32_t* strong_begin, int32_t* strong_end,
                        int32_t* node_weak, int32_t* node_strong);
+
+/* Outputs of pbb_bound_children_ex (host arrays; NULL = not wanted):
+ * everything pbb_bound_children returns, plus the children's idle-time
+ * priorities of the weak bound (prioBegin / prioEnd of
+ * bound_fsp_weak::boundChildren, bounds/src/bound_fsp_weak.cpp:134-221) and
+ * per node the idle time bound_fsp_strong::bornes_calculer returns in
+ * couts[1] (bounds/src/bound_fsp_strong.cpp:457-509, 541-560: 0 when nothing
+ * is fixed at the back, and 0 where the reference leaves it unset -- at most
+ * one free job). */
+typedef struct pbb_bound_out {
+    int32_t *weak_begin, *weak_end, *strong_begin, *strong_end;   /* count x n, by job id */
+    int32_t *node_weak, *node_strong;                             /* count */
+    int32_t *prio_begin, *prio_end;                               /* count x n, by job id */
+    int32_t *strong_idle;                                         /* count */
+} pbb_bound_out;
+
+int pbb_bound_children_ex(const pbb_instance* inst, int32_t johnson_mode, int32_t device, int32_t count,
+                          const int32_t* sched, const int32_t* limit1, const int32_t* limit2, const pbb_bound_out* out);
 
 /* pbb_bound_children for callers that cannot allocate GPU memory (a plugin
  * handed only device buffers, code running inside another framework's memory

@@ -60,6 +60,7 @@ def lib():
         L.orc_weak_children.argtypes = [ctypes.c_void_p, _i32p, ctypes.c_int, ctypes.c_int, ctypes.c_int,
                                         _i32p, _i32p, _i32p, _i32p]
         L.orc_strong_node.argtypes = [ctypes.c_void_p, _i32p, ctypes.c_int, ctypes.c_int]
+        L.orc_strong_idle.argtypes = [ctypes.c_void_p, _i32p, ctypes.c_int, ctypes.c_int]
         L.orc_johnson_row.argtypes = [ctypes.c_void_p, ctypes.c_int, _i32p]
         L.orc_lag_row.argtypes = [ctypes.c_void_p, ctypes.c_int, _i32p]
         L.orc_min_times.argtypes = [ctypes.c_void_p, _i32p, _i32p]
@@ -125,6 +126,11 @@ class Oracle:
 
     def strong_node(self, sched, l1, l2):
         return lib().orc_strong_node(self._h, _ptr(np.ascontiguousarray(sched, dtype=np.int32)), l1, l2)
+
+    def strong_node_idle(self, sched, l1, l2):
+        """couts[1] of the Johnson bound: idle time of the fixed jobs' schedules
+        (0 when nothing is fixed at the back or at most one job is free)."""
+        return lib().orc_strong_idle(self._h, _ptr(np.ascontiguousarray(sched, dtype=np.int32)), l1, l2)
 
     def strong_children(self, sched, l1, l2, front):
         """Johnson LB of every free job appended at the front (or back), by job id."""
@@ -207,6 +213,7 @@ class Reference:
             L.ref_weak_node.argtypes = [_i32p, ctypes.c_int, ctypes.c_int]
             L.ref_weak_children.argtypes = [_i32p, ctypes.c_int, ctypes.c_int, _i32p, _i32p, _i32p, _i32p]
             L.ref_strong_node.argtypes = [_i32p, ctypes.c_int, ctypes.c_int]
+            L.ref_strong_node_idle.argtypes = [_i32p, ctypes.c_int, ctypes.c_int, ctypes.c_int]
             L.ref_johnson_row.argtypes = [ctypes.c_int, _i32p]
             L.ref_children_batch.argtypes = [ctypes.c_int, ctypes.c_int, _i32p, _i32p, _i32p, _i32p, _i32p,
                                              _i32p, _i32p, _i32p, _i32p]
@@ -240,6 +247,11 @@ class Reference:
 
     def strong_node(self, sched, l1, l2):
         return Reference._L.ref_strong_node(_ptr(np.ascontiguousarray(sched, dtype=np.int32)), l1, l2)
+
+    def strong_node_idle(self, sched, l1, l2, unset=-1):
+        """couts[1] of the reference's Johnson bornes_calculer (`unset` where it
+        leaves the value untouched: at most one free job)."""
+        return Reference._L.ref_strong_node_idle(_ptr(np.ascontiguousarray(sched, dtype=np.int32)), l1, l2, unset)
 
     def johnson_row(self, s):
         out = np.zeros(self.n, np.int32)

@@ -1,8 +1,8 @@
 #!/usr/bin/env python3
 """Build the reference's own CPU code into oracle/_ref/ (test infrastructure).
 
-This recipe compiles jangmys/PBBPerm sources where they lie (read-only tree,
-default /root/reference, override with PBB_REFERENCE) from a scratch copy
+This recipe compiles jangmys/PBBPerm sources where they lie (read-only tree:
+PBB_REFERENCE, else a `reference` directory beside the repository) from a scratch copy
 under /tmp, with g++ invoked directly on the source files (the reference's own
 makefiles are not used).  Outputs, all git-ignored:
 
@@ -11,6 +11,9 @@ makefiles are not used).  Outputs, all git-ignored:
   oracle/_ref/testBounds         bounds/test/testBounds.cpp (known-answer tool)
   oracle/_ref/bb                 multicore/ B&B, weak re-evaluation as shipped
   oracle/_ref/bbJ                multicore/ B&B with the Johnson call restored
+  oracle/_ref/abstract_driver    oracle/abstract_driver.cpp: the engine's bounds adapter
+                                 derived from the reference's bound_abstract (its header and
+                                 bounds/src/bound_abstract.cpp), linked with libpbbperm.so
 
 Patches applied to the scratch copy (the shipped tree does not compile):
   P1 common/include/arguments.h + common/src/arguments.cpp: declare/define
@@ -35,7 +38,8 @@ import tempfile
 
 HERE = os.path.dirname(os.path.abspath(__file__))
 OUT = os.path.join(HERE, "_ref")
-REF = os.environ.get("PBB_REFERENCE", "/root/reference")
+# the reference tree: PBB_REFERENCE, else a `reference` directory beside the repository
+REF = os.environ.get("PBB_REFERENCE", os.path.join(os.path.dirname(os.path.dirname(HERE)), "reference"))
 
 
 def _patch(path, old, new, count=1):
@@ -110,6 +114,13 @@ def build(verbose=False):
                "bound[WEAK]->bornes_calculer(node->schedule, _limit1, _limit2, costs, arguments::earlyStopJohnson?local_best:-1);",
                "bound[STRONG]->bornes_calculer(node->schedule, _limit1, _limit2, costs, arguments::earlyStopJohnson?local_best:-1);")
         _run(["g++"] + flags + ["-o", os.path.join(OUT, "bbJ")] + srcs + inc + ["-lpthread", "-lm", "-ldl"], tmp)
+        # the bounds adapter as a bound_abstract (needs the engine library built)
+        pkg = os.path.join(os.path.dirname(HERE), "pbbperm_b200")
+        if os.path.exists(os.path.join(pkg, "libpbbperm.so")):
+            _run(["g++", "-O1", "-std=c++17", "-o", os.path.join(OUT, "abstract_driver"),
+                  os.path.join(HERE, "abstract_driver.cpp"), os.path.join(tmp, "bounds/src/bound_abstract.cpp"),
+                  "-I", os.path.join(tmp, "bounds/include"), "-I", os.path.join(os.path.dirname(HERE), "include"),
+                  "-L", pkg, "-lpbbperm", "-Wl,-rpath,$ORIGIN/../../pbbperm_b200"], tmp)
         if verbose:
             print("reference checker built into", OUT)
     finally:

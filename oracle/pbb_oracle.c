@@ -891,3 +891,33 @@ int orc_ig(const orc_inst *I, int iterations, int destruct, int destruct_max, in
     memcpy(perm, best, sizeof(int) * n);
     return best_cost;
 }
+
+/* couts[1] of bound_fsp_strong::bornes_calculer (bound_fsp_strong.cpp:541-560):
+ * the idle time of the front jobs' schedule (scheduleFront :457-478; 0 when
+ * nothing is fixed in front) plus that of the back jobs' (scheduleBack
+ * :490-509), all reset to 0 when nothing is fixed at the back; 0 with at most
+ * one free job, where the reference leaves the value as it was. */
+int orc_strong_idle(const orc_inst *I, const int *s, int l1, int l2)
+{
+    int n = I->n, m = I->m;
+    if (l2 - l1 <= 2 || l2 == n) return 0;
+    int fr[ORC_MAXM], bk[ORC_MAXM], idle = 0;
+    for (int k = 0; k < m; k++) { fr[k] = 0; bk[k] = 0; }
+    for (int i = 0; i <= l1; i++) {
+        int j = s[i];
+        fr[0] += I->p[j];
+        for (int k = 1; k < m; k++) {
+            idle += imax(0, fr[k - 1] - fr[k]);
+            fr[k] = imax(fr[k], fr[k - 1]) + I->p[k * n + j];
+        }
+    }
+    for (int i = n - 1; i >= l2; i--) {
+        int j = s[i];
+        bk[m - 1] += I->p[(m - 1) * n + j];
+        for (int k = m - 2; k >= 0; k--) {
+            idle += imax(0, bk[k + 1] - bk[k]);
+            bk[k] = imax(bk[k], bk[k + 1]) + I->p[k * n + j];
+        }
+    }
+    return idle;
+}

@@ -86,6 +86,16 @@ int ref_strong_node(const int* sched, int l1, int l2) {
     return c[0];
 }
 
+// couts[1] of bound_fsp_strong::bornes_calculer (idle time of the fixed
+// jobs' schedules); `unset` is returned where the reference leaves it as it was.
+int ref_strong_node_idle(const int* sched, int l1, int l2, int unset) {
+    int c[2] = {0, unset};
+    int tmp[1024];
+    memcpy(tmp, sched, g_n * sizeof(int));
+    g_strong->bornes_calculer(tmp, l1, l2, c, -1);
+    return c[1];
+}
+
 // Johnson order of machine pair s (bounds/src/bound_fsp_strong.cpp:343-354).
 void ref_johnson_row(int s, int* out) {
     memcpy(out, bound_fsp_strong::tabJohnson + s * g_n, g_n * sizeof(int));

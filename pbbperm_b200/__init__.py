@@ -89,6 +89,11 @@ class _PoolResult(ctypes.Structure):
                 ("result", _Result)]
 
 
+class _BoundOut(ctypes.Structure):
+    _fields_ = [(k, _i32p) for k in ("weak_begin", "weak_end", "strong_begin", "strong_end", "node_weak",
+                                     "node_strong", "prio_begin", "prio_end", "strong_idle")]
+
+
 _lib = None
 
 
@@ -111,6 +116,8 @@ def lib():
         L.pbb_bound_children.argtypes = [ctypes.POINTER(_Instance), ctypes.c_int32, ctypes.c_int32, ctypes.c_int32,
                                          _i32p, _i32p, _i32p, _i32p, _i32p, _i32p, _i32p, _i32p, _i32p]
         L.pbb_neh.argtypes = [ctypes.POINTER(_Instance), _i32p, _i32p]
+        L.pbb_bound_children_ex.argtypes = [ctypes.POINTER(_Instance), ctypes.c_int32, ctypes.c_int32,
+                                            ctypes.c_int32, _i32p, _i32p, _i32p, ctypes.POINTER(_BoundOut)]
         L.pbb_neh_batch.argtypes = [ctypes.POINTER(_Instance), ctypes.c_int32, ctypes.c_int32, _i32p, _i32p]
         L.pbb_ig_batch.argtypes = [ctypes.POINTER(_Instance), ctypes.c_int32, ctypes.c_int32, ctypes.c_int32,
                                    ctypes.c_uint64, _i32p, _i32p]
@@ -395,6 +402,26 @@ def decimal_to_fact(n, decimal):
     d = np.zeros(n, np.int32)
     _check(lib().pbb_decimal_to_fact(int(n), str(decimal).encode(), _ptr(d)))
     return d
+
+
+def bound_children_ex(p, sched, limit1, limit2, johnson_mode=0, device=0):
+    """bound_children plus the weak bound's idle-time priorities of every
+    child (prio_begin / prio_end, (count, n) by job id) and the Johnson
+    bound's couts[1] per node (strong_idle)."""
+    inst, p = _instance(p)
+    n = p.shape[1]
+    sched = np.ascontiguousarray(sched, dtype=np.int32).reshape(-1, n)
+    cnt = sched.shape[0]
+    l1 = np.ascontiguousarray(limit1, dtype=np.int32).reshape(cnt)
+    l2 = np.ascontiguousarray(limit2, dtype=np.int32).reshape(cnt)
+    out = {k: np.zeros((cnt, n), np.int32) for k in ("weak_begin", "weak_end", "strong_begin", "strong_end",
+                                                      "prio_begin", "prio_end")}
+    for k in ("node_weak", "node_strong", "strong_idle"):
+        out[k] = np.zeros(cnt, np.int32)
+    o = _BoundOut(**{k: _ptr(v) for k, v in out.items()})
+    _check(lib().pbb_bound_children_ex(ctypes.byref(inst), johnson_mode, device, cnt, _ptr(sched), _ptr(l1),
+                                       _ptr(l2), ctypes.byref(o)))
+    return out
 
 
 def int32_peak(device=0):

@@ -9,6 +9,7 @@ best value kept before the next is tried):
   core_warps              warps per CTA that always ask for work (steal threshold)
   split_depth             no split deeper than n - split_depth (steal threshold)
   explorers_per_instance  explorers of each resident instance (0 = one per warp of the widest grid)
+  window_s                device time of a window while instances wait (admission granularity)
 
 The sample is every k-th instance plus the largest ones (jobs x machines):
 a batch ends with its heaviest searches, which a uniform sample misses.
@@ -24,6 +25,7 @@ CANDIDATES = [
     ("core_warps", (8, 4)),
     ("split_depth", (10, 6, 14)),
     ("explorers_per_instance", (0, 1024)),
+    ("window_s", (0.01, 0.004, 0.02)),
 ]
 
 
@@ -35,8 +37,7 @@ def calibration_sample(instances, ubs, size=32, largest=2):
     return [instances[i] for i in idx], [ubs[i] for i in idx]
 
 
-def tune_pool(instances, ubs, search, max_jobs, max_machines, sample=32, window_s=0.01, device=0, repeats=1,
-              largest=2):
+def tune_pool(instances, ubs, search, max_jobs, max_machines, sample=32, device=0, repeats=1, largest=2):
     cal, cal_ub = calibration_sample(instances, ubs, sample, largest)
     current = {k: v[0] for k, v in CANDIDATES}
     trials = []
@@ -46,7 +47,7 @@ def tune_pool(instances, ubs, search, max_jobs, max_machines, sample=32, window_
         key = tuple(sorted(cfg.items()))
         if key in cache:
             return cache[key]
-        pc = pb.PoolConfig(max_jobs=max_jobs, max_machines=max_machines, window_s=window_s, device=device, **cfg)
+        pc = pb.PoolConfig(max_jobs=max_jobs, max_machines=max_machines, device=device, **cfg)
         t = float("inf")
         for _ in range(repeats):
             t0 = time.perf_counter()
@@ -63,5 +64,5 @@ def tune_pool(instances, ubs, search, max_jobs, max_machines, sample=32, window_
             t = timed(trial)
             if t < best_t:
                 best_t, current = t, trial
-    pc = pb.PoolConfig(max_jobs=max_jobs, max_machines=max_machines, window_s=window_s, device=device, **current)
+    pc = pb.PoolConfig(max_jobs=max_jobs, max_machines=max_machines, device=device, **current)
     return pc, trials

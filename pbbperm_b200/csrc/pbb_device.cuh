@@ -17,10 +17,21 @@
 #define NEG_INF (-(1 << 28))
 // at most this many children are bounded by direct scans instead of sweeps
 #define PBB_DIRECT_MAX 4
+// a lone child gets its own one-chain direct scan (instead of two chains, one
+// repeating the other)
+#ifndef PBB_DIRECT_ONE
+#define PBB_DIRECT_ONE 0
+#endif
+// unroll factor of the loop that builds a pair's free-position mask
+#ifndef PBB_FREEPOS_UNROLL
+#define PBB_FREEPOS_UNROLL 1
+#endif
 // Loops over machines and over free jobs stay rolled: the explorer kernel is
 // large and instruction-fetch bound, and unrolled copies of these loops cost
 // more in fetch stalls than they save in loop overhead.
 #define PBB_ROLLED _Pragma("unroll 1")
+#define PBB_PRAGMA(x) _Pragma(#x)
+#define PBB_UNROLL(n) PBB_PRAGMA(unroll n)
 
 namespace pbb {
 
@@ -552,7 +563,7 @@ __device__ __forceinline__ typename PosMask<NW>::type free_positions(const CtaTa
     typedef typename PosMask<NW>::type M;
     const unsigned char* col = T.posj + i;
     M pm = 0;
-    PBB_ROLLED
+    PBB_UNROLL(PBB_FREEPOS_UNROLL)
     for (int q = 0; q < k; q++) pm |= (M)1 << col[S.rowj[q] * T.Ppad];
     return pm;
 }
@@ -657,6 +668,10 @@ __device__ __forceinline__ void johnson_direct_masked(const CtaTables& T, const 
 {
     static_assert(PBB_DIRECT_MAX <= 4, "direct scans walk at most four children together");
     if (nc <= 0) return;
+#if PBB_DIRECT_ONE
+    if (nc == 1) johnson_direct_chains<1, NW>(T, S, k, nc, cjob, cside, stop);
+    else
+#endif
     if (nc <= 2) johnson_direct_chains<2, NW>(T, S, k, nc, cjob, cside, stop);
     else johnson_direct_chains<4, NW>(T, S, k, nc, cjob, cside, stop);
 }

@@ -763,7 +763,8 @@ int pbb_solve(pbb_engine* e, int32_t ub, const int32_t* root_perm, double time_l
 static int bound_children_impl(const pbb_instance* inst, int32_t johnson_mode, int32_t device, int32_t method,
                                int32_t count, const int32_t* sched, const int32_t* limit1, const int32_t* limit2,
                                int32_t* weak_begin, int32_t* weak_end, int32_t* strong_begin, int32_t* strong_end,
-                               int32_t* node_weak, int32_t* node_strong);
+                               int32_t* node_weak, int32_t* node_strong, int32_t* prio_begin = nullptr,
+                               int32_t* prio_end = nullptr, int32_t* strong_idle = nullptr);
 
 int pbb_bound_children(const pbb_instance* inst, int32_t johnson_mode, int32_t device, int32_t count,
                        const int32_t* sched, const int32_t* limit1, const int32_t* limit2, int32_t* weak_begin,
@@ -772,6 +773,15 @@ int pbb_bound_children(const pbb_instance* inst, int32_t johnson_mode, int32_t d
 {
     return bound_children_impl(inst, johnson_mode, device, 0, count, sched, limit1, limit2, weak_begin, weak_end,
                                strong_begin, strong_end, node_weak, node_strong);
+}
+
+int pbb_bound_children_ex(const pbb_instance* inst, int32_t johnson_mode, int32_t device, int32_t count,
+                          const int32_t* sched, const int32_t* limit1, const int32_t* limit2, const pbb_bound_out* out)
+{
+    if (!out) return fail(PBB_E_INVAL, "out is NULL");
+    return bound_children_impl(inst, johnson_mode, device, 0, count, sched, limit1, limit2, out->weak_begin,
+                               out->weak_end, out->strong_begin, out->strong_end, out->node_weak, out->node_strong,
+                               out->prio_begin, out->prio_end, out->strong_idle);
 }
 
 int pbb_diag_bound_children(const pbb_instance* inst, int32_t johnson_mode, int32_t device, int32_t method,
@@ -788,7 +798,8 @@ int pbb_diag_bound_children(const pbb_instance* inst, int32_t johnson_mode, int3
 static int bound_children_impl(const pbb_instance* inst, int32_t johnson_mode, int32_t device, int32_t method,
                                int32_t count, const int32_t* sched, const int32_t* limit1, const int32_t* limit2,
                                int32_t* weak_begin, int32_t* weak_end, int32_t* strong_begin, int32_t* strong_end,
-                               int32_t* node_weak, int32_t* node_strong)
+                               int32_t* node_weak, int32_t* node_strong, int32_t* prio_begin, int32_t* prio_end,
+                               int32_t* strong_idle)
 {
     if (count < 0 || (count > 0 && (!sched || !limit1 || !limit2))) return fail(PBB_E_INVAL, "bad node arrays");
     HostTables H;
@@ -814,7 +825,8 @@ static int bound_children_impl(const pbb_instance* inst, int32_t johnson_mode, i
     int* buf = nullptr;
     unsigned* status = nullptr;
     const size_t cn = (size_t)count * n;
-    const size_t words = cn * 5 + (size_t)count * 4;
+    const bool want_prio = prio_begin || prio_end;
+    const size_t words = cn * 5 + (size_t)count * 4 + (want_prio ? 2 * cn : 0) + (strong_idle ? count : 0);
     do {
         if (rc) break;
         cudaError_t ce = cudaMalloc(&buf, sizeof(int) * words);
@@ -829,6 +841,10 @@ static int bound_children_impl(const pbb_instance* inst, int32_t johnson_mode, i
         int* d_l2 = d_l1 + count;
         int* d_nw = d_l2 + count;
         int* d_ns = d_nw + count;
+        BoundExtra X;
+        int* tail = d_ns + count;
+        if (want_prio) { X.prio_begin = tail; X.prio_end = tail + cn; tail += 2 * cn; }
+        if (strong_idle) X.strong_idle = tail;
         cudaMemcpyAsync(d_s, sched, sizeof(int) * cn, cudaMemcpyHostToDevice, st);
         cudaMemcpyAsync(d_l1, limit1, sizeof(int) * count, cudaMemcpyHostToDevice, st);
         cudaMemcpyAsync(d_l2, limit2, sizeof(int) * count, cudaMemcpyHostToDevice, st);
@@ -841,7 +857,7 @@ static int bound_children_impl(const pbb_instance* inst, int32_t johnson_mode, i
         int ctas = (count + warps - 1) / warps;
         ctas = std::min(ctas, sms * 4);
         ce = pbbl::launch_bound(n <= 32 ? 1 : 2, di.view, count, d_s, d_l1, d_l2, d_wb, d_we, d_sb, d_se, d_nw, d_ns,
-                                status, ctas, warps, smem, st, method);
+                                status, ctas, warps, smem, st, method, X);
         if (ce != cudaSuccess) { rc = cuda_fail(ce, "pbb_bound_kernel launch"); break; }
         if (weak_begin) cudaMemcpyAsync(weak_begin, d_wb, sizeof(int) * cn, cudaMemcpyDeviceToHost, st);
         if (weak_end) cudaMemcpyAsync(weak_end, d_we, sizeof(int) * cn, cudaMemcpyDeviceToHost, st);
@@ -849,6 +865,9 @@ static int bound_children_impl(const pbb_instance* inst, int32_t johnson_mode, i
         if (strong_end) cudaMemcpyAsync(strong_end, d_se, sizeof(int) * cn, cudaMemcpyDeviceToHost, st);
         if (node_weak) cudaMemcpyAsync(node_weak, d_nw, sizeof(int) * count, cudaMemcpyDeviceToHost, st);
         if (node_strong) cudaMemcpyAsync(node_strong, d_ns, sizeof(int) * count, cudaMemcpyDeviceToHost, st);
+        if (prio_begin) cudaMemcpyAsync(prio_begin, X.prio_begin, sizeof(int) * cn, cudaMemcpyDeviceToHost, st);
+        if (prio_end) cudaMemcpyAsync(prio_end, X.prio_end, sizeof(int) * cn, cudaMemcpyDeviceToHost, st);
+        if (strong_idle) cudaMemcpyAsync(strong_idle, X.strong_idle, sizeof(int) * count, cudaMemcpyDeviceToHost, st);
         unsigned hs = 0;
         cudaMemcpyAsync(&hs, status, sizeof(unsigned), cudaMemcpyDeviceToHost, st);
         ce = cudaStreamSynchronize(st);

@@ -857,7 +857,7 @@ __global__ void pbb_lower_ub_kernel(const DevGroup* groups, int g, int ub)
 template <int NW>
 __global__ void pbb_bound_kernel(DevInstance I, int count, const int* sched, const int* l1s, const int* l2s,
                                  int* wb, int* we, int* sb, int* se, int* node_weak, int* node_strong,
-                                 unsigned int* status, int warps_per_cta, int method)
+                                 unsigned int* status, int warps_per_cta, int method, BoundExtra X)
 {
     extern __shared__ __align__(16) unsigned char smem[];
     const SmemPlan sp = pbb_smem_plan(I.n, I.m, I.Ppad, warps_per_cta);
@@ -902,6 +902,49 @@ __global__ void pbb_bound_kernel(DevInstance I, int count, const int* sched, con
                 owb[row[w]] = weak_front(T, S, row[w]);
                 owe[row[w]] = weak_back(T, S, row[w]);
             }
+        }
+        if (X.prio_begin) {
+            // idle-time priorities of the children (bound_fsp_weak.cpp:140-146, 172-178)
+            int* opb = X.prio_begin + (size_t)node * n;
+            int* ope = X.prio_end + (size_t)node * n;
+            for (int i = lane; i < n; i += 32) { opb[i] = 0; ope[i] = 0; }
+            __syncwarp();
+#pragma unroll
+            for (int w = 0; w < NW; w++) {
+                if (valid[w]) {
+                    opb[row[w]] = weak_front_idle(T, S, row[w]);
+                    ope[row[w]] = weak_back_idle(T, S, row[w]);
+                }
+            }
+        }
+        if (X.strong_idle && lane == 0) {
+            // couts[1] of bound_fsp_strong::bornes_calculer: idle time of the
+            // fixed jobs' schedules (scheduleFront :457-478, scheduleBack
+            // :490-509): 0 with nothing fixed in front for the front part, and
+            // 0 altogether when nothing is fixed at the back; 0 as well with at
+            // most one free job (the reference leaves it unset there)
+            int idle = 0;
+            if (k > 1 && b > 0) {
+                int fr[PBB_MAX_M], bk[PBB_MAX_M];
+                for (int q = 0; q < T.m; q++) { fr[q] = 0; bk[q] = 0; }
+                for (int i = 0; i < f; i++) {
+                    const int j = S.fjob[i];
+                    fr[0] += T.p[j];
+                    for (int q = 1; q < T.m; q++) {
+                        idle += max(0, fr[q - 1] - fr[q]);
+                        fr[q] = max(fr[q], fr[q - 1]) + T.p[q * n + j];
+                    }
+                }
+                for (int i = 0; i < b; i++) {
+                    const int j = S.bjob[i];
+                    bk[T.m - 1] += T.p[(T.m - 1) * n + j];
+                    for (int q = T.m - 2; q >= 0; q--) {
+                        idle += max(0, bk[q + 1] - bk[q]);
+                        bk[q] = max(bk[q], bk[q + 1]) + T.p[q * n + j];
+                    }
+                }
+            }
+            X.strong_idle[node] = idle;
         }
         const int wn = weak_node_lb(T, S);
         // node Johnson LB and children Johnson LBs
@@ -1068,16 +1111,16 @@ cudaError_t launch_explore(int nw, const DevGroup* groups, const int* ngroups_d,
 
 cudaError_t launch_bound(int nw, const DevInstance& I, int count, const int* sched, const int* l1, const int* l2,
                          int* wb, int* we, int* sb, int* se, int* nweak, int* nstrong, unsigned int* status,
-                         int ctas, int warps_per_cta, int smem, cudaStream_t st, int method)
+                         int ctas, int warps_per_cta, int smem, cudaStream_t st, int method, BoundExtra extra)
 {
     if (nw == 1) {
         cudaFuncSetAttribute(pbb_bound_kernel<1>, cudaFuncAttributeMaxDynamicSharedMemorySize, smem);
         pbb_bound_kernel<1><<<ctas, 32 * warps_per_cta, smem, st>>>(I, count, sched, l1, l2, wb, we, sb, se, nweak,
-                                                                     nstrong, status, warps_per_cta, method);
+                                                                     nstrong, status, warps_per_cta, method, extra);
     } else {
         cudaFuncSetAttribute(pbb_bound_kernel<2>, cudaFuncAttributeMaxDynamicSharedMemorySize, smem);
         pbb_bound_kernel<2><<<ctas, 32 * warps_per_cta, smem, st>>>(I, count, sched, l1, l2, wb, we, sb, se, nweak,
-                                                                     nstrong, status, warps_per_cta, method);
+                                                                     nstrong, status, warps_per_cta, method, extra);
     }
     return cudaGetLastError();
 }

@@ -20,5 +20,5 @@ cudaError_t launch_explore(int nw, const DevGroup* groups, const int* ngroups_d,
 int explore_ctas_per_sm(int nw, int warps_per_cta, int smem, int variant = 0);
 cudaError_t launch_bound(int nw, const DevInstance& I, int count, const int* sched, const int* l1, const int* l2,
                          int* wb, int* we, int* sb, int* se, int* nweak, int* nstrong, unsigned int* status, int ctas,
-                         int warps_per_cta, int smem, cudaStream_t st, int method = 0);
+                         int warps_per_cta, int smem, cudaStream_t st, int method = 0, BoundExtra extra = BoundExtra());
 }  // namespace pbbl

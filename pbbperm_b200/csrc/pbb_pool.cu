@@ -313,8 +313,11 @@ int pool_create(const pbb_pool_config* in, pbb_pool* P)
     if (P->tail_warps > 0) {
         graph = nullptr;
         PCK(cudaStreamBeginCapture(P->st, cudaStreamCaptureModeRelaxed), "graph capture");
+        // the tail's windows last at least 20 ms: its few long searches gain
+        // nothing from frequent admissions
+        const unsigned long long tail_budget = std::max(budget, 20000000ull);
         e1 = pbbl::launch_explore(P->nw, P->groups_d, P->ngroups_d, P->tail_grid, P->tail_warps, P->tail_smem,
-                                  budget, INT_MAX, 4096, P->st);
+                                  tail_budget, INT_MAX, 4096, P->st);
         e3 = cudaMemcpyAsync(P->ctl_h, P->ctl, sizeof(GroupCtl) * S, cudaMemcpyDeviceToHost, P->st);
         e4 = cudaStreamEndCapture(P->st, &graph);
         if (e1 || e3 || e4) {

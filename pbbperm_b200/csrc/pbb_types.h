@@ -123,6 +123,15 @@ struct DevGroup {
     SampleBuf* sample;     // NULL unless node sampling is armed
 };
 
+// Optional outputs of the bound kernel (NULL = not wanted): per node and job,
+// the children's idle-time priorities, and per node the Johnson bound's idle
+// time of the fixed jobs.
+struct BoundExtra {
+    int* prio_begin = nullptr;   // [count][n]
+    int* prio_end = nullptr;     // [count][n]
+    int* strong_idle = nullptr;  // [count]
+};
+
 // Dynamic shared memory layout of one CTA (host and device agree).
 struct SmemPlan {
     int je_off, p_off, pm0_off, pm1_off, marr_off, mdep_off, posj_off, warp_off, warp_bytes, total;

@@ -118,3 +118,60 @@ def test_shim_matches_the_oracle(tmp_path):
         assert [int(x) for x in lines[5 * i + 2].split()] == list(ce)
         assert [int(x) for x in lines[5 * i + 3].split()] == list(O.strong_children(perm, l1, l2, True))
         assert [int(x) for x in lines[5 * i + 4].split()] == list(O.strong_children(perm, l1, l2, False))
+
+
+def _reference_tree():
+    ref = os.environ.get("PBB_REFERENCE", os.path.join(os.path.dirname(ROOT), "reference"))
+    return ref if os.path.isdir(os.path.join(ref, "bounds", "include")) else None
+
+
+def test_adapter_derives_from_the_reference_bound_abstract():
+    """With the reference's bound_abstract.h included first, the header's
+    bound_fsp_gpu_abstract derives from it (compile check)."""
+    ref = _reference_tree()
+    if ref is None or not shutil.which("g++"):
+        pytest.skip("reference tree or g++ not available")
+    src = os.path.join(ROOT, "oracle", "abstract_driver.cpp")
+    r = subprocess.run(["g++", "-std=c++17", "-fsyntax-only", "-I", os.path.join(ref, "bounds", "include"),
+                        "-I", INC, src], stdout=subprocess.PIPE, stderr=subprocess.STDOUT, text=True)
+    assert r.returncode == 0, r.stdout
+
+
+@pytest.mark.gpu
+def test_adapter_through_the_reference_base_class():
+    """oracle/_ref/abstract_driver (built with the reference's bound_abstract)
+    calls the GPU bounds through bound_abstract pointers: node LBs, couts[1],
+    weak children with their priorities, Johnson children -- all equal to the
+    oracle's."""
+    exe = os.path.join(ROOT, "oracle", "_ref", "abstract_driver")
+    if not os.path.exists(exe):
+        pytest.skip("abstract driver not built (oracle/build_ref.py)")
+    n, m = 18, 9
+    p = synthetic_instance(62, n, m)
+    O = Oracle(p)
+    rng = np.random.default_rng(62)
+    nodes = []
+    for _ in range(30):
+        perm = rng.permutation(n).astype(np.int32)
+        nf = int(rng.integers(0, n))
+        nb = int(rng.integers(0, n - nf + 1))
+        l1, l2 = nf - 1, n - nb
+        if l1 < l2:
+            nodes.append((l1, l2, perm))
+    text = "%d %d\n%s\n%d\n" % (n, m, " ".join(str(v) for v in p.reshape(-1)), len(nodes))
+    text += "".join("%d %d %s\n" % (l1, l2, " ".join(map(str, perm))) for l1, l2, perm in nodes)
+    r = subprocess.run([exe], input=text, stdout=subprocess.PIPE, stderr=subprocess.STDOUT, text=True, timeout=300)
+    assert r.returncode == 0, r.stdout
+    lines = r.stdout.strip().splitlines()
+    assert len(lines) == 7 * len(nodes)
+    for i, (l1, l2, perm) in enumerate(nodes):
+        w, s, idle, mk = map(int, lines[7 * i].split())
+        assert w == O.weak_node(perm, l1, l2) and s == O.strong_node(perm, l1, l2) and mk == O.eval(perm)
+        assert idle == (O.strong_node_idle(perm, l1, l2) if l2 - l1 > 2 else -1)
+        cb, ce, pb_, pe_ = O.weak_children(perm, l1, l2)
+        got = [[int(x) for x in lines[7 * i + r].split()] for r in range(1, 7)]
+        free = perm[l1 + 1:l2]
+        assert got[0] == list(cb) and got[1] == list(ce)
+        assert [got[2][j] for j in free] == list(pb_[free]) and [got[3][j] for j in free] == list(pe_[free])
+        assert got[4] == list(O.strong_children(perm, l1, l2, True))
+        assert got[5] == list(O.strong_children(perm, l1, l2, False))

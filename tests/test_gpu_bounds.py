@@ -87,3 +87,29 @@ def test_lb_agreement_large_sample():
     for i in range(0, len(sched), 997):
         assert (g["strong_begin"][i] == O.strong_children(sched[i], l1[i], l2[i], True)).all()
         assert (g["strong_end"][i] == O.strong_children(sched[i], l1[i], l2[i], False)).all()
+
+
+@pytest.mark.parametrize("n,m,seed", [(20, 20, 1), (50, 20, 2), (9, 4, 3)])
+def test_bound_children_ex_priorities_and_idle(n, m, seed):
+    """pbb_bound_children_ex: the weak bound's idle-time priorities of every
+    child and the Johnson bound's couts[1] per node, bit-exact with the
+    reference bounds library (the oracle when it is not built)."""
+    import oracle
+    p = synthetic_instance(seed, n, m)
+    rng = np.random.default_rng(seed + 100)
+    sched, l1, l2 = random_nodes(rng, n, 400)
+    g = pb.bound_children_ex(p, sched, l1, l2)
+    chk = oracle.Reference(p) if oracle.reference_available() else Oracle(p)
+    O = Oracle(p)
+    for i in range(len(sched)):
+        _, _, pbw, pew = chk.weak_children(sched[i], l1[i], l2[i])
+        free = sched[i, l1[i] + 1:l2[i]]
+        assert (g["prio_begin"][i][free] == pbw[free]).all() and (g["prio_end"][i][free] == pew[free]).all()
+        fixed = np.setdiff1d(np.arange(n), free)
+        assert (g["prio_begin"][i][fixed] == 0).all() and (g["prio_end"][i][fixed] == 0).all()
+        if isinstance(chk, oracle.Reference):
+            want = chk.strong_node_idle(sched[i], l1[i], l2[i], unset=0)
+        else:
+            want = O.strong_node_idle(sched[i], l1[i], l2[i])
+        assert g["strong_idle"][i] == want
+        assert (g["weak_begin"][i] == O.weak_children(sched[i], l1[i], l2[i])[0]).all()

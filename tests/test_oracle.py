@@ -131,3 +131,28 @@ def test_neh_is_a_valid_upper_bound():
         assert sorted(perm.tolist()) == list(range(n))
         assert O.eval(perm) == c
         assert c >= O.strong_node(np.arange(n), -1, n)
+
+
+def test_oracle_priorities_and_idle_vs_reference_library():
+    """The weak bound's idle-time priorities (prioBegin / prioEnd) and the
+    Johnson bound's couts[1] of the oracle equal the reference bounds
+    library's on random nodes (what pbb_bound_children_ex returns)."""
+    if not oracle.reference_available():
+        pytest.skip("reference checker not built")
+    for seed, n, m in [(71, 12, 6), (72, 20, 20), (73, 33, 5)]:
+        p = synthetic_instance(seed, n, m)
+        O, R = Oracle(p), oracle.Reference(p)
+        rng = np.random.default_rng(seed)
+        for _ in range(60):
+            s = rng.permutation(n).astype(np.int32)
+            nf = int(rng.integers(0, n))
+            nb = int(rng.integers(0, n - nf + 1))
+            l1, l2 = nf - 1, n - nb
+            if l1 >= l2:
+                continue
+            _, _, opb, ope = O.weak_children(s, l1, l2)
+            _, _, rpb, rpe = R.weak_children(s, l1, l2)
+            free = s[l1 + 1:l2]
+            assert (opb[free] == rpb[free]).all() and (ope[free] == rpe[free]).all()
+            want = R.strong_node_idle(s, l1, l2, unset=0)
+            assert O.strong_node_idle(s, l1, l2) == want, (seed, l1, l2)
