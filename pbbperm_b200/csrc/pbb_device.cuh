@@ -15,8 +15,13 @@
 
 #define FULLMASK 0xffffffffu
 #define NEG_INF (-(1 << 28))
-// at most this many children are bounded by direct scans instead of sweeps
+// direct scans walk at most this many children together
 #define PBB_DIRECT_MAX 4
+// nodes with at most this many Johnson children use direct scans (by groups
+// of PBB_DIRECT_MAX), more children use the max-plus sweeps
+#ifndef PBB_DIRECT_LIMIT
+#define PBB_DIRECT_LIMIT 4
+#endif
 // a lone child gets its own one-chain direct scan (instead of two chains, one
 // repeating the other)
 #ifndef PBB_DIRECT_ONE
@@ -971,7 +976,44 @@ __device__ __forceinline__ int bound_and_prune(const CtaTables& T, const WarpScr
                     if (w * 32 + lane < PBB_MAX_N) { S.lbF[w * 32 + lane] = 0; S.lbB[w * 32 + lane] = 0; }
                 }
                 child_tables<NW>(T, S, row, k, nF > 0, sF, nB > 0, sB);
-                if (nF + nB <= PBB_DIRECT_MAX) {
+                if (nF + nB <= PBB_DIRECT_LIMIT) {
+#if PBB_DIRECT_LIMIT > PBB_DIRECT_MAX
+                    // list the children (front side first, job order), then
+                    // scan them by groups of at most PBB_DIRECT_MAX
+                    int list[PBB_DIRECT_LIMIT];
+                    int nc = 0;
+#pragma unroll
+                    for (int side = 0; side < 2; side++) {
+#pragma unroll
+                        for (int q = 0; q < NW; q++) {
+                            unsigned msk = side ? sB[q] : sF[q];
+                            while (msk) {
+                                const int j = q * 32 + __ffs(msk) - 1;
+                                msk &= msk - 1;
+#pragma unroll
+                                for (int c = 0; c < PBB_DIRECT_LIMIT; c++)
+                                    if (nc == c) list[c] = j | (side << 8);
+                                nc++;
+                            }
+                        }
+                    }
+                    // the early exit lives in the runtime-options build only (SORT = 1):
+                    // the default explorer passes a constant and keeps no trace of it
+                    const int stop = (SORT && srch.early_stop) ? best : INT_MAX;
+                    PBB_ROLLED
+                    for (int g = 0; g < nc; g += PBB_DIRECT_MAX) {
+                        int cjob[4] = {0, 0, 0, 0}, cside[4] = {0, 0, 0, 0};
+#pragma unroll
+                        for (int c = 0; c < 4; c++) {
+#pragma unroll
+                            for (int e = 0; e < PBB_DIRECT_LIMIT; e++)
+                                if (e == g + c) { cjob[c] = list[e] & 0xff; cside[c] = list[e] >> 8; }
+                        }
+                        const int gn = min(nc - g, PBB_DIRECT_MAX);
+                        if (T.posj) johnson_direct_masked<NW>(T, S, k, gn, cjob, cside, stop);
+                        else johnson_direct<NW>(T, S, um, gn, cjob, cside);
+                    }
+#else
                     // list the children (front side first, job order)
                     int cjob[4] = {0, 0, 0, 0}, cside[4] = {0, 0, 0, 0};
                     int nc = 0;
@@ -995,6 +1037,7 @@ __device__ __forceinline__ int bound_and_prune(const CtaTables& T, const WarpScr
                     const int stop = (SORT && srch.early_stop) ? best : INT_MAX;
                     if (T.posj) johnson_direct_masked<NW>(T, S, k, nc, cjob, cside, stop);
                     else johnson_direct<NW>(T, S, um, nc, cjob, cside);
+#endif
                     cnt.direct_children += nc;
                     cnt.direct_free += (unsigned long long)nc * k;
                 } else {
