@@ -128,8 +128,8 @@ struct CtaTables {
 };
 
 struct WarpScratch {
-    int* lbF;     // [64] Johnson LB of front children, by job
-    int* lbB;     // [64]
+    int* lbF;     // [n] Johnson LB of front children, by job
+    int* lbB;     // [n]
     int* frontZ;  // [32] heads of the front jobs (zero based)
     int* backZ;   // [32] tails of the back jobs (zero based)
     int* Fb;      // [32] front used by the bounds (earliest starts when no front job)
@@ -137,19 +137,28 @@ struct WarpScratch {
     int* rem;     // [32] machine loads of the free jobs
     int* RB;      // [32] rem + Bb
     int* FR;      // [32] Fb + rem
-    short* dF;    // [64][m] heads of front child u minus frontZ
-    short* dB;    // [64][m] tails of back child u minus backZ
-    unsigned char* fjob;  // [64] front jobs in schedule order
-    unsigned char* bjob;  // [64] back jobs, last position first
-    unsigned char* rowj;  // [64] free jobs (row order)
+    short* dF;    // [n][m] heads of front child u minus frontZ
+    short* dB;    // [n][m] tails of back child u minus backZ
+    unsigned char* fjob;  // [n] front jobs in schedule order
+    unsigned char* bjob;  // [n] back jobs, last position first
+    unsigned char* rowj;  // [n] free jobs (row order)
+    // [Ppad] per machine pair, the Johnson positions of the free jobs of the
+    // explorer this warp holds (bit t = position t), kept up to date by the
+    // explorer as it moves; NULL outside the explorer or when it does not fit
+    unsigned long long* fmask;
 };
 
-__device__ __forceinline__ WarpScratch warp_scratch(unsigned char* base, int m)
+__device__ __forceinline__ WarpScratch warp_scratch(unsigned char* base, const SmemPlan& sp, int n, int m, int Ppad)
 {
     WarpScratch s;
+    s.fmask = nullptr;
+    if (sp.fmask) {
+        s.fmask = reinterpret_cast<unsigned long long*>(base);
+        base += Ppad * 8;
+    }
     int* ip = reinterpret_cast<int*>(base);
-    s.lbF = ip; ip += PBB_MAX_N;
-    s.lbB = ip; ip += PBB_MAX_N;
+    s.lbF = ip; ip += n;
+    s.lbB = ip; ip += n;
     s.frontZ = ip; ip += 32;
     s.backZ = ip; ip += 32;
     s.Fb = ip; ip += 32;
@@ -157,12 +166,12 @@ __device__ __forceinline__ WarpScratch warp_scratch(unsigned char* base, int m)
     s.rem = ip; ip += 32;
     s.RB = ip; ip += 32;
     s.FR = ip; ip += 32;
-    short* sp = reinterpret_cast<short*>(ip);
-    s.dF = sp; sp += PBB_MAX_N * m;
-    s.dB = sp; sp += PBB_MAX_N * m;
-    unsigned char* bp = reinterpret_cast<unsigned char*>(sp);
-    s.fjob = bp; bp += PBB_MAX_N;
-    s.bjob = bp; bp += PBB_MAX_N;
+    short* sp2 = reinterpret_cast<short*>(ip);
+    s.dF = sp2; sp2 += n * m;
+    s.dB = sp2; sp2 += n * m;
+    unsigned char* bp = reinterpret_cast<unsigned char*>(sp2);
+    s.fjob = bp; bp += n;
+    s.bjob = bp; bp += n;
     s.rowj = bp;
     return s;
 }
@@ -573,6 +582,41 @@ __device__ __forceinline__ typename PosMask<NW>::type free_positions(const CtaTa
     return pm;
 }
 
+// The free-position masks of the explorer a warp holds (S.fmask, explorer
+// only): built from the row at its line when the warp takes the explorer,
+// then kept exact by flipping one bit per machine pair as it moves: going
+// down removes the chosen job, going up puts back the job of the level it
+// returns to.  The bound then reads one word per pair instead of rebuilding
+// the mask from the k free jobs at every node.
+template <int NW>
+__device__ __forceinline__ void fmask_build(const CtaTables& T, const WarpScratch& S, const int (&row)[NW], int k)
+{
+#pragma unroll
+    for (int w = 0; w < NW; w++) {
+        const int idx = w * 32 + lane_id();
+        if (idx < k) S.rowj[idx] = (unsigned char)cell_job(row[w]);
+    }
+    __syncwarp();
+    for (int i = lane_id(); i < T.P; i += 32) S.fmask[i] = (unsigned long long)free_positions<NW>(T, S, k, i);
+    __syncwarp();
+}
+
+__device__ __forceinline__ void fmask_flip(const CtaTables& T, const WarpScratch& S, int u)
+{
+    const unsigned char* col = T.posj + u * T.Ppad;
+    for (int i = lane_id(); i < T.P; i += 32) S.fmask[i] ^= 1ull << col[i];
+    __syncwarp();
+}
+
+// the free-position mask of pair i for the node being bounded
+template <int NW>
+__device__ __forceinline__ typename PosMask<NW>::type node_positions(const CtaTables& T, const WarpScratch& S, int k,
+                                                                     int i)
+{
+    typedef typename PosMask<NW>::type M;
+    return S.fmask ? (M)S.fmask[i] : free_positions<NW>(T, S, k, i);
+}
+
 // Scan start of child u on pair (m0, m1): front child = heads of front + u,
 // remaining back as is; back child = heads of front, tails of u + back.
 __device__ __forceinline__ void direct_start(const CtaTables& T, const WarpScratch& S, int u, int side, int m0, int m1,
@@ -630,7 +674,7 @@ __device__ __forceinline__ void johnson_direct_chains(const CtaTables& T, const 
                 direct_start(T, S, u[c], sd[c], m0, m1, t0[c], t1[c], B0[c], B1[c]);
                 px[c] = T.posj[u[c] * T.Ppad + i];
             }
-            M pm = free_positions<NW>(T, S, k, i);
+            M pm = node_positions<NW>(T, S, k, i);
             const unsigned long long* col = T.je + i;
             while (pm) {
                 const int t = low_pos(pm);
@@ -703,7 +747,7 @@ __device__ __forceinline__ void johnson_sweep_masked(const CtaTables& T, const W
             const int cB3 = S.Fb[m0] + Asum + S.backZ[m0];
             const unsigned long long* col = T.je + i;
             typedef typename PosMask<NW>::type M;
-            const M pm = free_positions<NW>(T, S, k, i);
+            const M pm = node_positions<NW>(T, S, k, i);
             int Apre = 0, Bpre = 0, PMx = NEG_INF;
             M fwd = pm;
             while (fwd) {
@@ -973,7 +1017,7 @@ __device__ __forceinline__ int bound_and_prune(const CtaTables& T, const WarpScr
             } else {
 #pragma unroll
                 for (int w = 0; w < NW; w++) {
-                    if (w * 32 + lane < PBB_MAX_N) { S.lbF[w * 32 + lane] = 0; S.lbB[w * 32 + lane] = 0; }
+                    if (w * 32 + lane < T.n) { S.lbF[w * 32 + lane] = 0; S.lbB[w * 32 + lane] = 0; }
                 }
                 child_tables<NW>(T, S, row, k, nF > 0, sF, nB > 0, sB);
                 if (nF + nB <= PBB_DIRECT_LIMIT) {

@@ -86,13 +86,20 @@ int max_smem_optin(int dev)
     return v;
 }
 
-int pick_warps(const HostTables& H, int requested, int dev, int& smem)
+// The most warps per CTA (up to `requested`) whose tables and scratch fit;
+// `explorer`: add the per-warp free-position masks when they fit too (the
+// explorer runs one CTA per SM, so they never cost a warp).
+int pick_warps(const HostTables& H, int requested, int dev, int& smem, bool explorer = false)
 {
     const int cap = max_smem_optin(dev);
     int w = requested > 0 ? std::min(requested, PBB_WARPS_MAX) : PBB_WARPS_MAX;
     for (; w >= 1; w--) {
         smem = pbbl::smem_bytes(H.n, H.m, H.Ppad, w);
-        if (smem <= cap) return w;
+        if (smem <= cap) {
+            const int with_masks = pbbl::smem_bytes(H.n, H.m, H.Ppad, w, 1);
+            if (explorer && with_masks <= cap) smem = with_masks;
+            return w;
+        }
     }
     return 0;
 }
@@ -305,7 +312,7 @@ static int engine_create(const pbb_instance* inst, const pbb_config* cfg, pbb_en
     CK(cudaEventCreate(&e->ev1));
     const HostTables& H = e->H;
     e->nw = H.n <= 32 ? 1 : 2;
-    e->warps = pick_warps(H, cfg->warps_per_cta, e->dev, e->smem);
+    e->warps = pick_warps(H, cfg->warps_per_cta, e->dev, e->smem, true);
     if (e->warps < 1) return fail(PBB_E_INVAL, "instance tables do not fit in shared memory");
     e->root_smem = pbbl::smem_bytes(H.n, H.m, H.Ppad, 1);
     int sms = 0;

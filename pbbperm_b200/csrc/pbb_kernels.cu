@@ -253,6 +253,7 @@ __device__ __forceinline__ int select_node(const DevGroup& G, const CtaTables& T
                 vset<NW>(R.pos, L, 0);
                 L--;
                 R.line = L;
+                if (S.fmask) fmask_flip(T, S, vget<NW>(R.pj, L));   // its job is free again
                 load_row<NW>(G.ivm, id, L, R.row);
                 load_path<NW>(G.ivm, id, L, R);
                 const int pp = vget<NW>(R.pos, L);
@@ -278,6 +279,7 @@ __device__ __forceinline__ int select_node(const DevGroup& G, const CtaTables& T
         C.decomposed++;
         const int u = vget<NW>(R.row, p);
         vset<NW>(R.pj, L, u);
+        if (S.fmask) fmask_flip(T, S, u);                  // u is fixed below this level
         path_down<NW>(T, R, u, vget<NW>(R.dir, L));
         int nr[NW];
 #pragma unroll
@@ -625,7 +627,7 @@ __global__ void pbb_root_kernel(const DevGroup* groups, int ngroups, const int* 
     CtaTables T;
     load_tables(G.inst, smem, sp, T);
     __syncthreads();
-    const WarpScratch S = warp_scratch(smem + sp.warp_off, T.m);
+    const WarpScratch S = warp_scratch(smem + sp.warp_off, sp, T.n, T.m, T.Ppad);
     const int n = T.n;
     const int id = ids ? ids[b] : b % per_group;
     Ivm<NW> R;
@@ -722,12 +724,18 @@ pbb_explore_kernel(const DevGroup* groups, const int* ngroups_d, int warps_per_c
     const int gi = group_of_cta(groups, ngroups);
     const DevGroup G = groups[gi];
     if ((int)blockIdx.x >= G.first_cta + G.ctas) return;
-    const SmemPlan sp = pbb_smem_plan(G.inst.n, G.inst.m, G.inst.Ppad, warps_per_cta);
+    // each warp keeps its explorer's free-position masks when the launch
+    // gave the room for them (the host sizes the launch with them if they fit)
+    unsigned dyn_smem;
+    asm("mov.u32 %0, %%dynamic_smem_size;" : "=r"(dyn_smem));
+    const int fm = G.inst.posj != nullptr &&
+                   pbb_smem_plan(G.inst.n, G.inst.m, G.inst.Ppad, warps_per_cta, 1).total <= (int)dyn_smem;
+    const SmemPlan sp = pbb_smem_plan(G.inst.n, G.inst.m, G.inst.Ppad, warps_per_cta, fm);
     CtaTables T;
     load_tables(G.inst, smem, sp, T);
     __syncthreads();
     const int wic = threadIdx.x >> 5;
-    const WarpScratch S = warp_scratch(smem + sp.warp_off + wic * sp.warp_bytes, T.m);
+    const WarpScratch S = warp_scratch(smem + sp.warp_off + wic * sp.warp_bytes, sp, T.n, T.m, T.Ppad);
     const int W = G.ctas * warps_per_cta;
     const int wid = (blockIdx.x - G.first_cta) * warps_per_cta + wic;
     const int mode = G.search.bound_mode;
@@ -782,6 +790,7 @@ pbb_explore_kernel(const DevGroup* groups, const int* ngroups_d, int warps_per_c
                 if (st == IVM_ACTIVE) {
                     load_ivm<NW>(G.ivm, id, R);
                     cached = id;
+                    if (S.fmask) fmask_build<NW>(T, S, R.row, T.n - R.line);
                 } else {
                     id = -1;
                 }
@@ -865,7 +874,7 @@ __global__ void pbb_bound_kernel(DevInstance I, int count, const int* sched, con
     load_tables(I, smem, sp, T);
     __syncthreads();
     const int wic = threadIdx.x >> 5;
-    const WarpScratch S = warp_scratch(smem + sp.warp_off + wic * sp.warp_bytes, T.m);
+    const WarpScratch S = warp_scratch(smem + sp.warp_off + wic * sp.warp_bytes, sp, T.n, T.m, T.Ppad);
     const int n = T.n;
     const int lane = lane_id();
     for (int node = blockIdx.x * warps_per_cta + wic; node < count; node += gridDim.x * warps_per_cta) {
@@ -979,7 +988,7 @@ __global__ void pbb_bound_kernel(DevInstance I, int count, const int* sched, con
                     }
                 }
             }
-            for (int i = lane; i < PBB_MAX_N; i += 32) { S.lbF[i] = 0; S.lbB[i] = 0; }
+            for (int i = lane; i < T.n; i += 32) { S.lbF[i] = 0; S.lbB[i] = 0; }
             __syncwarp();
             const bool kids = k >= 3;
             unsigned none[NW];
@@ -1036,7 +1045,7 @@ __global__ void pbb_bound_kernel(DevInstance I, int count, const int* sched, con
 // ---------------------------------------------------------------------------
 namespace pbbl {
 
-int smem_bytes(int n, int m, int Ppad, int warps) { return pbb_smem_plan(n, m, Ppad, warps).total; }
+int smem_bytes(int n, int m, int Ppad, int warps, int fmask) { return pbb_smem_plan(n, m, Ppad, warps, fmask).total; }
 
 template <int NW, int VAR>
 int explore_occupancy(int warps_per_cta, int smem)

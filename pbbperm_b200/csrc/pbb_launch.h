@@ -4,7 +4,9 @@
 #include "pbb_types.h"
 
 namespace pbbl {
-int smem_bytes(int n, int m, int Ppad, int warps);
+// dynamic shared memory of a CTA; fmask = 1 adds the explorer's per-warp
+// free-position masks
+int smem_bytes(int n, int m, int Ppad, int warps, int fmask = 0);
 cudaError_t launch_reset(const DevGroup* groups, int ngroups, const int* ub, cudaStream_t st);
 // reset must run first; interval b = g * per_group + j starts explorer j of
 // group g, or explorer ids[b] when ids is given (distinct, < the explorer count)

@@ -242,8 +242,13 @@ int pool_create(const pbb_pool_config* in, pbb_pool* P)
     cudaDeviceGetAttribute(&optin, cudaDevAttrMaxSharedMemoryPerBlockOptin, P->dev);
     cudaDeviceGetAttribute(&sms, cudaDevAttrMultiProcessorCount, P->dev);
     if (P->smem > optin) return pfail(PBB_E_INVAL, "tables of max_jobs x max_machines do not fit in shared memory");
-    const int per_sm = pbbl::explore_ctas_per_sm(P->nw, P->warps, P->smem);
+    int per_sm = pbbl::explore_ctas_per_sm(P->nw, P->warps, P->smem);
     if (per_sm < 1) return pfail(PBB_E_INVAL, "explorer kernel cannot be resident with this block shape");
+    {
+        // per-warp free-position masks, when they cost no resident CTA
+        const int ms = pbbl::smem_bytes(c.max_jobs, c.max_machines, P->Ppad_max, P->warps, 1);
+        if (ms <= optin && pbbl::explore_ctas_per_sm(P->nw, P->warps, ms) >= per_sm) P->smem = ms;
+    }
     // every window launches all the CTAs the GPU holds at once and spreads
     // them over the resident instances
     int capacity = sms * per_sm;
@@ -253,8 +258,10 @@ int pool_create(const pbb_pool_config* in, pbb_pool* P)
     // searches that finish last want every warp an SM holds)
     const int tw = c.tail_warps == 0 ? PBB_WARPS_MAX : c.tail_warps;
     if (tw > P->warps && tw <= PBB_WARPS_MAX) {
-        const int ts = pbbl::smem_bytes(c.max_jobs, c.max_machines, P->Ppad_max, tw);
+        int ts = pbbl::smem_bytes(c.max_jobs, c.max_machines, P->Ppad_max, tw);
         const int tper = ts <= optin ? pbbl::explore_ctas_per_sm(P->nw, tw, ts) : 0;
+        const int tms = pbbl::smem_bytes(c.max_jobs, c.max_machines, P->Ppad_max, tw, 1);
+        if (tper >= 1 && tms <= optin && pbbl::explore_ctas_per_sm(P->nw, tw, tms) >= tper) ts = tms;
         if (tper >= 1) {
             P->tail_warps = tw;
             P->tail_smem = ts;

@@ -135,13 +135,19 @@ struct BoundExtra {
 // Dynamic shared memory layout of one CTA (host and device agree).
 struct SmemPlan {
     int je_off, p_off, pm0_off, pm1_off, marr_off, mdep_off, posj_off, warp_off, warp_bytes, total;
+    int fmask;             // 1: each warp keeps its explorer's free-position masks (explorer only)
 };
 
 __host__ __device__ inline int pbb_align(int x, int a) { return (x + a - 1) / a * a; }
 
-// per-warp scratch: ints lbF[64] lbB[64] frontZ backZ Fb Bb rem RB FR [32 each];
-// shorts dF[64*m] dB[64*m]; bytes fjob[64] bjob[64] row[64]
-__host__ __device__ inline SmemPlan pbb_smem_plan(int n, int m, int Ppad, int warps)
+// per-warp scratch: [fmask: u64 fmask[Ppad]] ints lbF[n] lbB[n] frontZ backZ
+// Fb Bb rem RB FR [32 each]; shorts dF[n*m] dB[n*m]; bytes fjob[n] bjob[n] row[n]
+__host__ __device__ inline int pbb_warp_bytes(int n, int m, int Ppad, int fmask)
+{
+    return pbb_align((fmask ? Ppad * 8 : 0) + (2 * n + 7 * 32) * 4 + 2 * n * m * 2 + 3 * n, 16);
+}
+
+__host__ __device__ inline SmemPlan pbb_smem_plan(int n, int m, int Ppad, int warps, int fmask = 0)
 {
     SmemPlan s;
     int off = 0;
@@ -153,7 +159,8 @@ __host__ __device__ inline SmemPlan pbb_smem_plan(int n, int m, int Ppad, int wa
     s.mdep_off = off; off += pbb_align(m * 4, 16);
     s.posj_off = off; off += pbb_align(n * Ppad, 16);
     s.warp_off = off;
-    s.warp_bytes = pbb_align((2 * PBB_MAX_N + 7 * 32) * 4 + 2 * PBB_MAX_N * m * 2 + 3 * PBB_MAX_N, 16);
+    s.fmask = fmask;
+    s.warp_bytes = pbb_warp_bytes(n, m, Ppad, fmask);
     off += s.warp_bytes * warps;
     s.total = off;
     return s;
