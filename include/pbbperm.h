@@ -86,6 +86,10 @@ typedef struct pbb_config {
     int32_t core_warps;         /* work sharing: warps per CTA that ask for work whatever the search's
                                    width; the others join once it is wide (0 = 8) */
     int32_t split_depth;        /* work sharing: no split at levels deeper than n - split_depth (0 = 10) */
+    int32_t share_after;        /* work sharing: an explorer hands part of its interval to an idle one only
+                                   after decomposing this many nodes since it got its interval or last
+                                   gave part away (0 = 64; < 0 = at every step). Node counts do not
+                                   depend on it */
 } pbb_config;
 
 typedef struct pbb_stats {
@@ -210,6 +214,8 @@ typedef struct pbb_pool_config {
     int64_t explorer_bytes;      /* explorer memory budget (0 = 8 GiB) */
     int32_t core_warps;          /* work sharing of every instance, as pbb_config (0 = 8) */
     int32_t split_depth;         /* as pbb_config (0 = 10) */
+    int32_t share_after;         /* as pbb_config (0 = 64; < 0 = at every step) */
+    int32_t pad;
 } pbb_pool_config;
 
 typedef struct pbb_pool_result {

@@ -52,7 +52,7 @@ class _Config(ctypes.Structure):
                 ("nb_ivms", ctypes.c_int32), ("device", ctypes.c_int32),
                 ("warps_per_cta", ctypes.c_int32), ("ctas", ctypes.c_int32),
                 ("sorting_criterion", ctypes.c_int32), ("core_warps", ctypes.c_int32),
-                ("split_depth", ctypes.c_int32)]
+                ("split_depth", ctypes.c_int32), ("share_after", ctypes.c_int32)]
 
 
 class _Stats(ctypes.Structure):
@@ -81,7 +81,8 @@ class _PoolConfig(ctypes.Structure):
                 ("max_resident", ctypes.c_int32), ("warps_per_cta", ctypes.c_int32),
                 ("ctas_per_instance", ctypes.c_int32), ("explorers_per_instance", ctypes.c_int32),
                 ("tail_warps", ctypes.c_int32), ("window_s", ctypes.c_double), ("explorer_bytes", ctypes.c_int64),
-                ("core_warps", ctypes.c_int32), ("split_depth", ctypes.c_int32)]
+                ("core_warps", ctypes.c_int32), ("split_depth", ctypes.c_int32),
+                ("share_after", ctypes.c_int32), ("pad", ctypes.c_int32)]
 
 
 class _PoolResult(ctypes.Structure):
@@ -176,7 +177,7 @@ class Config:
 
     def __init__(self, boundingMode=2, adaptiveBranchingMode=3, findAll=False, JohnsonMode=0,
                  earlyStopJohnson=False, sortedDFS=0, nbIVMs=16384, device=0, warps_per_cta=0, ctas=0,
-                 sortingCriterion=1, core_warps=0, split_depth=0):
+                 sortingCriterion=1, core_warps=0, split_depth=0, share_after=0):
         self.boundingMode = boundingMode
         self.adaptiveBranchingMode = adaptiveBranchingMode
         self.findAll = findAll
@@ -190,11 +191,13 @@ class Config:
         self.sortingCriterion = sortingCriterion
         self.core_warps = core_warps
         self.split_depth = split_depth
+        self.share_after = share_after
 
     def _c(self):
         return _Config(self.boundingMode, self.adaptiveBranchingMode, 1 if self.findAll else 0, self.JohnsonMode,
                        1 if self.earlyStopJohnson else 0, self.sortedDFS, self.nbIVMs, self.device,
-                       self.warps_per_cta, self.ctas, self.sortingCriterion, self.core_warps, self.split_depth)
+                       self.warps_per_cta, self.ctas, self.sortingCriterion, self.core_warps, self.split_depth,
+                       self.share_after)
 
 
 def _result(r):
@@ -470,7 +473,7 @@ class PoolConfig:
 
     def __init__(self, max_jobs=32, max_machines=20, max_resident=0, warps_per_cta=8, ctas_per_instance=0,
                  explorers_per_instance=0, window_s=0.005, explorer_bytes=8 << 30, device=0, tail_warps=0,
-                 core_warps=0, split_depth=0):
+                 core_warps=0, split_depth=0, share_after=0):
         self.max_jobs = max_jobs
         self.max_machines = max_machines
         self.max_resident = max_resident
@@ -483,11 +486,12 @@ class PoolConfig:
         self.tail_warps = tail_warps
         self.core_warps = core_warps
         self.split_depth = split_depth
+        self.share_after = share_after
 
     def _c(self):
         return _PoolConfig(self.device, self.max_jobs, self.max_machines, self.max_resident, self.warps_per_cta,
                            self.ctas_per_instance, self.explorers_per_instance, self.tail_warps, self.window_s,
-                           self.explorer_bytes, self.core_warps, self.split_depth)
+                           self.explorer_bytes, self.core_warps, self.split_depth, self.share_after)
 
 
 class Pool:

@@ -8,6 +8,7 @@ best value kept before the next is tried):
   tail_warps              block shape once few instances remain (0 = 20 warps, -1 = none)
   core_warps              warps per CTA that always ask for work (steal threshold)
   split_depth             no split deeper than n - split_depth (steal threshold)
+  share_after             nodes an explorer decomposes before it offers work again (steal threshold)
   explorers_per_instance  explorers of each resident instance (0 = one per warp of the widest grid)
   window_s                device time of a window while instances wait (admission granularity)
 
@@ -24,6 +25,7 @@ CANDIDATES = [
     ("tail_warps", (0, -1)),
     ("core_warps", (8, 4)),
     ("split_depth", (10, 6, 14)),
+    ("share_after", (64, 16, 256)),
     ("explorers_per_instance", (0, 1024)),
     ("window_s", (0.01, 0.004, 0.02)),
 ]

@@ -363,6 +363,7 @@ static int engine_create(const pbb_instance* inst, const pbb_config* cfg, pbb_en
     g.search.sort_crit = cfg->sorting_criterion;
     g.search.core_warps = cfg->core_warps > 0 ? cfg->core_warps : PBB_CORE_WARPS;
     g.search.split_depth = cfg->split_depth > 0 ? cfg->split_depth : PBB_SPLIT_DEPTH;
+    g.search.share_after = cfg->share_after > 0 ? cfg->share_after : (cfg->share_after < 0 ? 0 : PBB_SHARE_AFTER);
     g.search.early_stop = cfg->early_stop_johnson ? 1 : 0;
     g.ivm.count = B;
     g.ivm.npad = npad;

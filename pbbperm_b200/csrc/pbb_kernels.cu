@@ -744,6 +744,7 @@ pbb_explore_kernel(const DevGroup* groups, const int* ngroups_d, int warps_per_c
     WarpCounters C = {0, 0, 0, 0, 0, 0, 0, 0, 0};
     Ivm<NW> R;
     int cached = -1;                   // explorer whose state is held in registers
+    int since = 0;                     // nodes it decomposed since it got work or gave some away
     // explorers holding work once the first core_warps warps of every CTA
     // are busy (no more than that share of the explorers can be)
     const int core_warps = G.search.core_warps;
@@ -790,6 +791,7 @@ pbb_explore_kernel(const DevGroup* groups, const int* ngroups_d, int warps_per_c
                 if (st == IVM_ACTIVE) {
                     load_ivm<NW>(G.ivm, id, R);
                     cached = id;
+                    since = 0;
                     if (S.fmask) fmask_build<NW>(T, S, R.row, T.n - R.line);
                 } else {
                     id = -1;
@@ -801,8 +803,14 @@ pbb_explore_kernel(const DevGroup* groups, const int* ngroups_d, int warps_per_c
             if (lane_id() == 0) gb = (int)(ld_volatile_u64(&G.ctl->best_key) >> 32);
             gb = __shfl_sync(FULLMASK, gb, 0);
             if (gb < best) best = gb;
-            try_share<NW>(G, id, R);
+            // an explorer offers work once it has decomposed share_after nodes
+            // since it got its interval or last split it: in a narrow tree,
+            // splitting at every step hands out pieces that end before they
+            // pay for the split, and keeps the donors splitting instead of
+            // exploring
+            if (since >= G.search.share_after && try_share<NW>(G, id, R) == 1) since = 0;
             const int r = select_node<NW>(G, T, S, id, R, best, C, select_budget);
+            if (r == 1) since++;
             if (r == 1) bound_current<NW, (VAR >= 1), (VAR == 2)>(G, T, S, id, R, mode, best, C);
             worked = true;
             if (r == 0) {

@@ -105,7 +105,7 @@ struct pbb_pool {
     int max_slots = 0;          // resident instances at most
     int grid = 0;               // CTAs of a window launch (all the CTAs of this shape the GPU holds)
     int tail_warps = 0, tail_grid = 0, tail_smem = 0;   // the tail's block shape (0 warps: none)
-    int core_warps = PBB_CORE_WARPS, split_depth = PBB_SPLIT_DEPTH;
+    int core_warps = PBB_CORE_WARPS, split_depth = PBB_SPLIT_DEPTH, share_after = PBB_SHARE_AFTER;
     int Ppad_max = 0;
     size_t table_stride = 0;
     size_t off_je = 0, off_p = 0, off_pm = 0, off_mt = 0, off_posj = 0;
@@ -234,6 +234,7 @@ int pool_create(const pbb_pool_config* in, pbb_pool* P)
     P->epw = c.explorers_per_instance;
     P->core_warps = c.core_warps > 0 ? c.core_warps : PBB_CORE_WARPS;
     P->split_depth = c.split_depth > 0 ? c.split_depth : PBB_SPLIT_DEPTH;
+    P->share_after = c.share_after > 0 ? c.share_after : (c.share_after < 0 ? 0 : PBB_SHARE_AFTER);
     const int Pmax = c.max_machines * (c.max_machines - 1) / 2;
     P->Ppad_max = (Pmax + 31) / 32 * 32;
     P->smem = pbbl::smem_bytes(c.max_jobs, c.max_machines, P->Ppad_max, P->warps);
@@ -451,6 +452,7 @@ int admit(pbb_pool* P, std::vector<int>& admitted)
         g.search.early_stop = 0;
         g.search.core_warps = P->core_warps;
         g.search.split_depth = P->split_depth;
+        g.search.share_after = P->share_after;
         carve_explorers(P->arena + off, E, P->npad, g.ivm);
         g.ctl = P->ctl + s;
         admitted.push_back(s);

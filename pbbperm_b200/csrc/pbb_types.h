@@ -7,6 +7,7 @@
 #define PBB_WARPS_MAX 20      // explorer warps per CTA (96 registers a thread)
 #define PBB_CORE_WARPS 8      // default of DevSearch::core_warps
 #define PBB_SPLIT_DEPTH 10    // default of DevSearch::split_depth
+#define PBB_SHARE_AFTER 64    // default of DevSearch::share_after
 
 // IVM life cycle (per explorer, in global memory)
 #define IVM_IDLE 0            // no interval
@@ -52,6 +53,8 @@ struct DevSearch {
     int early_stop;    // [bb] earlyStopJohnson: a child's Johnson scan may stop once it exceeds the incumbent
     int core_warps;    // warps per CTA that ask for work whatever the search's width (1..warps per CTA)
     int split_depth;   // work is not split at levels deeper than n - split_depth
+    int share_after;   // an explorer offers work only after decomposing this many nodes since it got
+                       // its interval or last gave part of it away (0 = at every step)
 };
 
 // Per-group control block (device memory).

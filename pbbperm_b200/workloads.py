@@ -64,7 +64,7 @@ def run_batch(count=512, pool_config=None, solo_sample=None, device=0):
                 solo_instances=len(idx), solo_seconds=t_solo, solo_inst_per_s=len(idx) / t_solo,
                 speedup=(count / t_batch) / (len(idx) / t_solo), all_verified=ok, same_optima_as_solo=same,
                 nodes=int(sum(r["decomposed"] for r in res)),
-                pool={k: getattr(pc, k) for k in ("warps_per_cta", "tail_warps", "core_warps", "split_depth",
+                pool={k: getattr(pc, k) for k in ("warps_per_cta", "tail_warps", "core_warps", "split_depth", "share_after",
                                                   "explorers_per_instance", "window_s")})
 
 

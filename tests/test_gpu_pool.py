@@ -34,10 +34,12 @@ def mix():
     return insts, ref
 
 
-def test_batch_counters_equal_solo(mix):
+@pytest.mark.parametrize("share_after", [0, -1, 16])
+def test_batch_counters_equal_solo(mix, share_after):
     insts, ref = mix
     res = pb.batch_solve(insts, ubs=[r["opt"] for r in ref], config=pb.Config(boundingMode=2),
-                         pool_config=pb.PoolConfig(max_jobs=12, max_machines=10, window_s=0.01))
+                         pool_config=pb.PoolConfig(max_jobs=12, max_machines=10, window_s=0.01,
+                                                   share_after=share_after))
     for i, (got, r) in enumerate(zip(res, ref)):
         assert got["complete"]
         for k in KEYS:

@@ -105,6 +105,19 @@ def test_counters_independent_of_explorer_count(ivms):
         assert got[k] == want[k], (ivms, k, got[k], want[k])
 
 
+@pytest.mark.parametrize("share_after", [-1, 1, 64, 5000])
+def test_counters_independent_of_share_threshold(share_after):
+    """How long an explorer works before it may hand work away changes who
+    explores what, never which nodes are decomposed: counters equal the
+    oracle's whether explorers split at every step (-1), after every node,
+    after 64 (the default) or almost never."""
+    p = synthetic_instance(24, 13, 20)
+    want = Oracle(p).solve(1803, bound_mode=2)
+    got = solve(p, 1803, ivms=4096, boundingMode=2, share_after=share_after)
+    for k in KEYS:
+        assert got[k] == want[k], (share_after, k, got[k], want[k])
+
+
 def test_windowed_exploration_matches_single_solve():
     p = synthetic_instance(24, 13, 20)
     want = Oracle(p).solve(1803, bound_mode=2)
@@ -156,10 +169,11 @@ def test_config2_20x20_johnson_ub_opt(config2_golden):
     UB = optimum 2352: decomposed-node count equals the reference's."""
     c = config2_golden
     p = synthetic_instance(c["seed"], c["n"], c["m"])
-    got = solve(p, c["opt"], ivms=16384, boundingMode=2)
-    assert got["complete"]
-    for k in KEYS:
-        assert got[k] == c[k], (k, got[k], c[k])
+    for share_after in (0, -1):
+        got = solve(p, c["opt"], ivms=16384, boundingMode=2, share_after=share_after)
+        assert got["complete"]
+        for k in KEYS:
+            assert got[k] == c[k], (share_after, k, got[k], c[k])
 
 
 @pytest.mark.parametrize("world", [2, 3])
