@@ -34,8 +34,8 @@ N_JOBS, N_MACH, SEED = 50, 20, 2
 NB_IVMS = 65536
 # explorer-kernel DRAM traffic (read + write) per second of window, from
 # `ncu --set full` on this workload (dram__bytes_read.sum + dram__bytes_write.sum
-# = 13.61 MB + 3.31 MB over a 50.1 ms launch)
-NCU_DRAM_BYTES_PER_S = (13.607936e6 + 3.314944e6) / 0.050112288
+# = 14.60 MB + 5.53 MB over a 50.1 ms launch)
+NCU_DRAM_BYTES_PER_S = (14.600448e6 + 5.531392e6) / 0.050105824
 BOUND_MODE, BRANCH_MODE = 2, 3
 METRIC = "decomposed nodes/s (50x20, Johnson LB)"
 
