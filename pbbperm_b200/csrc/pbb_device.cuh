@@ -944,7 +944,9 @@ __device__ __noinline__ void sort_cells(unsigned char* out, int k, unsigned long
 // Returns the side chosen for this level.  SAMPLE = 1 with `rec` set writes
 // the children's bounds, as computed and before pruning, into a node record
 // (SampleBuf layout: schedule at rec + PBB_SAMPLE_HDR, then four arrays of n).
-template <int NW, int SORT = 1, int SAMPLE = 0>
+// RULE != 0 fixes the branching rule at compile time (the caller then passes
+// a constant mode too), so the hot explorer carries no code for the others.
+template <int NW, int SORT = 1, int SAMPLE = 0, int RULE = 0>
 __device__ __forceinline__ int bound_and_prune(const CtaTables& T, const WarpScratch& S, const DevSearch& srch,
                                                int mode, int (&row)[NW], int k, int f, int b, int line,
                                                int prev_dir, int best, NodeCounters& cnt, bool partial_ready = false,
@@ -976,7 +978,7 @@ __device__ __forceinline__ int bound_and_prune(const CtaTables& T, const WarpScr
             }
         }
         cnt.simple += both ? 2 * k : k;
-        dir = choose_dir<NW>(srch.branch_mode, line, best, cbw, cew, valid);
+        dir = choose_dir<NW>(RULE ? RULE : srch.branch_mode, line, best, cbw, cew, valid);
     }
 
     if (mode != 0) {
@@ -1098,7 +1100,7 @@ __device__ __forceinline__ int bound_and_prune(const CtaTables& T, const WarpScr
                 }
             }
         }
-        if (mode == 1) dir = choose_dir<NW>(srch.branch_mode, line, best, cbs, ces, valid);
+        if (mode == 1) dir = choose_dir<NW>(RULE ? RULE : srch.branch_mode, line, best, cbs, ces, valid);
     }
 
     if (SAMPLE && rec) {

@@ -681,7 +681,8 @@ int pbb_explore(pbb_engine* e, double seconds, int32_t* done)
         const double win = (seconds > 0 && seconds < 120.0) ? seconds : 120.0;
         const unsigned long long budget = (unsigned long long)(win * 1e9);
         CK(cudaEventRecord(e->ev0, e->st));
-        const int variant = e->sample_d ? 2 : ((e->cfg.sorted_dfs || e->cfg.early_stop_johnson) ? 1 : 0);
+        int variant = e->sample_d ? 2 : ((e->cfg.sorted_dfs || e->cfg.early_stop_johnson) ? 1 : 0);
+        if (variant == 0 && e->cfg.bounding_mode == 2 && e->cfg.branching_mode == 3) variant = 3;
         CK(pbbl::launch_explore(e->nw, e->group_d, e->ngroups_d, e->ctas, e->warps, e->smem, budget, e->max_rounds,
                                 e->select_budget, e->st, variant));
         CK(cudaEventRecord(e->ev1, e->st));

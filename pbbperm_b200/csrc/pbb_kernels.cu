@@ -367,7 +367,7 @@ __device__ __forceinline__ int* sample_slot(const DevGroup& G, const WarpScratch
 }
 
 // Bound and prune the node selected at R.line and write its row back.
-template <int NW, int SORT, int SAMPLE>
+template <int NW, int SORT, int SAMPLE, int RULE>
 __device__ __forceinline__ void bound_current(const DevGroup& G, const CtaTables& T, const WarpScratch& S, int id,
                                               Ivm<NW>& R, int mode, int best, WarpCounters& C)
 {
@@ -378,7 +378,7 @@ __device__ __forceinline__ void bound_current(const DevGroup& G, const CtaTables
     int* rec = nullptr;
     if (SAMPLE) rec = sample_slot<NW>(G, S, R, id, f, b, best, C.decomposed);
     NodeCounters nc = {0, 0, 0, 0, 0};
-    const int d = bound_and_prune<NW, SORT, SAMPLE>(T, S, G.search, mode, R.row, T.n - L, f, b, L, prev, best, nc,
+    const int d = bound_and_prune<NW, SORT, SAMPLE, RULE>(T, S, G.search, mode, R.row, T.n - L, f, b, L, prev, best, nc,
                                                     true, rec);
     vset<NW>(R.dir, L, d);
     store_row<NW>(G.ivm, id, L, R.row);
@@ -706,7 +706,9 @@ __global__ void pbb_root_kernel(const DevGroup* groups, int ngroups, const int* 
 
 // Persistent explorer loop.  Warp w of a group serves explorers w, w+W, ...
 // (W = warps of the group).  Runs until no explorer of the group holds work,
-// or `budget_ns` of device time has passed, or `max_rounds` rounds.  VAR = 0
+// or `budget_ns` of device time has passed, or `max_rounds` rounds.  VAR = 3
+// is VAR 0 for boundingMode 2 with MinMin branching (the default search),
+// both compiled in as constants; VAR = 0
 // compiles the sortedDFS row sorts, the early Johnson exit and node sampling
 // out of the hot loop; VAR = 1 follows each group's sortedDFS and
 // earlyStopJohnson settings; VAR = 2 also records sampled nodes into the
@@ -738,7 +740,7 @@ pbb_explore_kernel(const DevGroup* groups, const int* ngroups_d, int warps_per_c
     const WarpScratch S = warp_scratch(smem + sp.warp_off + wic * sp.warp_bytes, sp, T.n, T.m, T.Ppad);
     const int W = G.ctas * warps_per_cta;
     const int wid = (blockIdx.x - G.first_cta) * warps_per_cta + wic;
-    const int mode = G.search.bound_mode;
+    const int mode = VAR == 3 ? 2 : G.search.bound_mode;
     const unsigned long long t0 = globaltimer_ns();
 
     WarpCounters C = {0, 0, 0, 0, 0, 0, 0, 0, 0};
@@ -811,7 +813,8 @@ pbb_explore_kernel(const DevGroup* groups, const int* ngroups_d, int warps_per_c
             if (since >= G.search.share_after && try_share<NW>(G, id, R) == 1) since = 0;
             const int r = select_node<NW>(G, T, S, id, R, best, C, select_budget);
             if (r == 1) since++;
-            if (r == 1) bound_current<NW, (VAR >= 1), (VAR == 2)>(G, T, S, id, R, mode, best, C);
+            if (r == 1)
+                bound_current<NW, (VAR == 1 || VAR == 2), (VAR == 2), (VAR == 3 ? 3 : 0)>(G, T, S, id, R, mode, best, C);
             worked = true;
             if (r == 0) {
                 // interval exhausted: leave the pool of busy explorers (the
@@ -1067,11 +1070,19 @@ int explore_occupancy(int warps_per_cta, int smem)
 int explore_ctas_per_sm(int nw, int warps_per_cta, int smem, int variant)
 {
     if (nw == 1) {
-        if (variant == 2) return explore_occupancy<1, 2>(warps_per_cta, smem);
-        return variant ? explore_occupancy<1, 1>(warps_per_cta, smem) : explore_occupancy<1, 0>(warps_per_cta, smem);
+        switch (variant) {
+        case 1: return explore_occupancy<1, 1>(warps_per_cta, smem);
+        case 2: return explore_occupancy<1, 2>(warps_per_cta, smem);
+        case 3: return explore_occupancy<1, 3>(warps_per_cta, smem);
+        default: return explore_occupancy<1, 0>(warps_per_cta, smem);
+        }
     }
-    if (variant == 2) return explore_occupancy<2, 2>(warps_per_cta, smem);
-    return variant ? explore_occupancy<2, 1>(warps_per_cta, smem) : explore_occupancy<2, 0>(warps_per_cta, smem);
+    switch (variant) {
+    case 1: return explore_occupancy<2, 1>(warps_per_cta, smem);
+    case 2: return explore_occupancy<2, 2>(warps_per_cta, smem);
+    case 3: return explore_occupancy<2, 3>(warps_per_cta, smem);
+    default: return explore_occupancy<2, 0>(warps_per_cta, smem);
+    }
 }
 
 cudaError_t launch_reset(const DevGroup* groups, int ngroups, const int* ub, cudaStream_t st)
@@ -1118,11 +1129,19 @@ cudaError_t launch_explore(int nw, const DevGroup* groups, const int* ngroups_d,
 #define PBB_EXPLORE(NW_, VAR_) \
     explore_launch<NW_, VAR_>(groups, ngroups_d, ctas, warps_per_cta, smem, budget_ns, max_rounds, select_budget, st)
     if (nw == 1) {
-        if (variant == 2) return PBB_EXPLORE(1, 2);
-        return variant ? PBB_EXPLORE(1, 1) : PBB_EXPLORE(1, 0);
+        switch (variant) {
+        case 1: return PBB_EXPLORE(1, 1);
+        case 2: return PBB_EXPLORE(1, 2);
+        case 3: return PBB_EXPLORE(1, 3);
+        default: return PBB_EXPLORE(1, 0);
+        }
     }
-    if (variant == 2) return PBB_EXPLORE(2, 2);
-    return variant ? PBB_EXPLORE(2, 1) : PBB_EXPLORE(2, 0);
+    switch (variant) {
+    case 1: return PBB_EXPLORE(2, 1);
+    case 2: return PBB_EXPLORE(2, 2);
+    case 3: return PBB_EXPLORE(2, 3);
+    default: return PBB_EXPLORE(2, 0);
+    }
 #undef PBB_EXPLORE
 }
 

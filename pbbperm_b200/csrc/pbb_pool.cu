@@ -124,6 +124,7 @@ struct pbb_pool {
     NehTask* neh_tasks_d = nullptr;
     cudaGraphExec_t window = nullptr;
     cudaGraphExec_t window_tail = nullptr;   // the same window with the tail's block shape
+    cudaGraphExec_t window_fixed = nullptr, window_tail_fixed = nullptr;   // boundingMode 2 + MinMin builds
     std::vector<Slot> slots;
     // the FIFO and the finished results are shared with submitting and
     // polling threads; everything else belongs to the thread driving step()
@@ -156,6 +157,8 @@ extern "C" int pbb_pool_destroy(pbb_pool* P)
     if (P->st) cudaStreamSynchronize(P->st);
     if (P->window) cudaGraphExecDestroy(P->window);
     if (P->window_tail) cudaGraphExecDestroy(P->window_tail);
+    if (P->window_fixed) cudaGraphExecDestroy(P->window_fixed);
+    if (P->window_tail_fixed) cudaGraphExecDestroy(P->window_tail_fixed);
     cudaFree(P->arena);
     cudaFree(P->tables);
     cudaFree(P->ctl);
@@ -302,40 +305,39 @@ int pool_create(const pbb_pool_config* in, pbb_pool* P)
     PCK(cudaMalloc(&P->arena, P->arena_bytes), "explorer memory");
     P->alloc.init(P->arena_bytes);
     P->slots.assign(S, Slot());
-    // the window: explorer kernel and control read-back, as one graph
-    cudaGraph_t graph = nullptr;
+    // the window: explorer kernel and control read-back, as one graph; one
+    // graph per block shape (bulk, tail) and explorer build (the general one,
+    // and the one with boundingMode 2 and MinMin compiled in, used while every
+    // resident instance searches that way)
     const unsigned long long budget = (unsigned long long)(c.window_s * 1e9);
-    PCK(cudaStreamBeginCapture(P->st, cudaStreamCaptureModeRelaxed), "graph capture");
-    cudaError_t e1 = pbbl::launch_explore(P->nw, P->groups_d, P->ngroups_d, P->grid, P->warps, P->smem, budget,
-                                          INT_MAX, 4096, P->st);
-    cudaError_t e2 = cudaSuccess;
-    cudaError_t e3 = cudaMemcpyAsync(P->ctl_h, P->ctl, sizeof(GroupCtl) * S, cudaMemcpyDeviceToHost, P->st);
-    cudaError_t e4 = cudaStreamEndCapture(P->st, &graph);
-    if (e1 || e2 || e3 || e4) {
-        if (graph) cudaGraphDestroy(graph);
-        return pfail(PBB_E_CUDA, "capturing the window graph failed");
-    }
-    cudaError_t e5 = cudaGraphInstantiate(&P->window, graph, 0);
-    cudaGraphDestroy(graph);
-    if (e5) return pfail(PBB_E_CUDA, "instantiating the window graph failed");
-    if (P->tail_warps > 0) {
-        graph = nullptr;
+    // the tail's windows last at least 20 ms: its few long searches gain
+    // nothing from frequent admissions
+    const unsigned long long tail_budget = std::max(budget, 20000000ull);
+    auto capture = [&](int grid, int warps, int smem, unsigned long long win, int variant,
+                       cudaGraphExec_t* out) -> int {
+        cudaGraph_t graph = nullptr;
         PCK(cudaStreamBeginCapture(P->st, cudaStreamCaptureModeRelaxed), "graph capture");
-        // the tail's windows last at least 20 ms: its few long searches gain
-        // nothing from frequent admissions
-        const unsigned long long tail_budget = std::max(budget, 20000000ull);
-        e1 = pbbl::launch_explore(P->nw, P->groups_d, P->ngroups_d, P->tail_grid, P->tail_warps, P->tail_smem,
-                                  tail_budget, INT_MAX, 4096, P->st);
-        e3 = cudaMemcpyAsync(P->ctl_h, P->ctl, sizeof(GroupCtl) * S, cudaMemcpyDeviceToHost, P->st);
-        e4 = cudaStreamEndCapture(P->st, &graph);
+        cudaError_t e1 = pbbl::launch_explore(P->nw, P->groups_d, P->ngroups_d, grid, warps, smem, win, INT_MAX, 4096,
+                                              P->st, variant);
+        cudaError_t e3 = cudaMemcpyAsync(P->ctl_h, P->ctl, sizeof(GroupCtl) * P->slots.size(),
+                                         cudaMemcpyDeviceToHost, P->st);
+        cudaError_t e4 = cudaStreamEndCapture(P->st, &graph);
         if (e1 || e3 || e4) {
             if (graph) cudaGraphDestroy(graph);
-            return pfail(PBB_E_CUDA, "capturing the tail window graph failed");
+            return pfail(PBB_E_CUDA, "capturing a window graph failed");
         }
-        e5 = cudaGraphInstantiate(&P->window_tail, graph, 0);
+        cudaError_t e5 = cudaGraphInstantiate(out, graph, 0);
         cudaGraphDestroy(graph);
-        if (e5) return pfail(PBB_E_CUDA, "instantiating the tail window graph failed");
+        if (e5) return pfail(PBB_E_CUDA, "instantiating a window graph failed");
+        return PBB_OK;
+    };
+    int rc = capture(P->grid, P->warps, P->smem, budget, 0, &P->window);
+    if (!rc) rc = capture(P->grid, P->warps, P->smem, budget, 3, &P->window_fixed);
+    if (!rc && P->tail_warps > 0) {
+        rc = capture(P->tail_grid, P->tail_warps, P->tail_smem, tail_budget, 0, &P->window_tail);
+        if (!rc) rc = capture(P->tail_grid, P->tail_warps, P->tail_smem, tail_budget, 3, &P->window_tail_fixed);
     }
+    if (rc) return rc;
     return PBB_OK;
 }
 
@@ -555,7 +557,11 @@ extern "C" int pbb_pool_step(pbb_pool* P, int32_t* resident, int32_t* queued)
             "upload");
     }
     PCK(cudaMemcpyAsync(P->ngroups_d, &nact, sizeof(int), cudaMemcpyHostToDevice, P->st), "upload");
-    if (nact > 0) PCK(cudaGraphLaunch(tail ? P->window_tail : P->window, P->st), "window launch");
+    bool fixed = true;
+    for (int i = 0; i < nact; i++)
+        fixed = fixed && act[i].search.bound_mode == 2 && act[i].search.branch_mode == 3;
+    cudaGraphExec_t win = tail ? (fixed ? P->window_tail_fixed : P->window_tail) : (fixed ? P->window_fixed : P->window);
+    if (nact > 0) PCK(cudaGraphLaunch(win, P->st), "window launch");
     PCK(cudaStreamSynchronize(P->st), "window");
     // retire the finished instances
     for (int i = 0; i < nact; i++) {
