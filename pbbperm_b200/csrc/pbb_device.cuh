@@ -608,12 +608,14 @@ __device__ __forceinline__ void fmask_flip(const CtaTables& T, const WarpScratch
     __syncwarp();
 }
 
-// the free-position mask of pair i for the node being bounded
-template <int NW>
+// the free-position mask of pair i for the node being bounded (FM: the
+// warp's masks are known to be there)
+template <int NW, int FM = 0>
 __device__ __forceinline__ typename PosMask<NW>::type node_positions(const CtaTables& T, const WarpScratch& S, int k,
                                                                      int i)
 {
     typedef typename PosMask<NW>::type M;
+    if (FM) return (M)S.fmask[i];
     return S.fmask ? (M)S.fmask[i] : free_positions<NW>(T, S, k, i);
 }
 
@@ -647,7 +649,7 @@ __device__ __forceinline__ void direct_start(const CtaTables& T, const WarpScrat
 // running maximum exceeds `stop` the remaining passes are skipped; such a
 // child is pruned whatever its remaining pairs give, so only the value of a
 // pruned child changes (INT_MAX = no early exit).
-template <int C, int NW>
+template <int C, int NW, int FM = 0>
 __device__ __forceinline__ void johnson_direct_chains(const CtaTables& T, const WarpScratch& S, int k, int nc,
                                                       const int (&cjob)[4], const int (&cside)[4], int stop)
 {
@@ -674,7 +676,7 @@ __device__ __forceinline__ void johnson_direct_chains(const CtaTables& T, const 
                 direct_start(T, S, u[c], sd[c], m0, m1, t0[c], t1[c], B0[c], B1[c]);
                 px[c] = T.posj[u[c] * T.Ppad + i];
             }
-            M pm = node_positions<NW>(T, S, k, i);
+            M pm = node_positions<NW, FM>(T, S, k, i);
             const unsigned long long* col = T.je + i;
             while (pm) {
                 const int t = low_pos(pm);
@@ -711,23 +713,23 @@ __device__ __forceinline__ void johnson_direct_chains(const CtaTables& T, const 
     __syncwarp();
 }
 
-template <int NW>
+template <int NW, int FM = 0>
 __device__ __forceinline__ void johnson_direct_masked(const CtaTables& T, const WarpScratch& S, int k, int nc,
                                                       const int (&cjob)[4], const int (&cside)[4], int stop)
 {
     static_assert(PBB_DIRECT_MAX <= 4, "direct scans walk at most four children together");
     if (nc <= 0) return;
 #if PBB_DIRECT_ONE
-    if (nc == 1) johnson_direct_chains<1, NW>(T, S, k, nc, cjob, cside, stop);
+    if (nc == 1) johnson_direct_chains<1, NW, FM>(T, S, k, nc, cjob, cside, stop);
     else
 #endif
-    if (nc <= 2) johnson_direct_chains<2, NW>(T, S, k, nc, cjob, cside, stop);
-    else johnson_direct_chains<4, NW>(T, S, k, nc, cjob, cside, stop);
+    if (nc <= 2) johnson_direct_chains<2, NW, FM>(T, S, k, nc, cjob, cside, stop);
+    else johnson_direct_chains<4, NW, FM>(T, S, k, nc, cjob, cside, stop);
 }
 
 // johnson_children (forward + backward max-plus sweeps) over the free
 // positions only (needs T.posj); same results, O(P k) instead of O(P n).
-template <int NW>
+template <int NW, int FM = 0>
 __device__ __forceinline__ void johnson_sweep_masked(const CtaTables& T, const WarpScratch& S, int k,
                                                      bool doF,
                                                      const unsigned (&sF)[NW], bool doB, const unsigned (&sB)[NW])
@@ -747,7 +749,7 @@ __device__ __forceinline__ void johnson_sweep_masked(const CtaTables& T, const W
             const int cB3 = S.Fb[m0] + Asum + S.backZ[m0];
             const unsigned long long* col = T.je + i;
             typedef typename PosMask<NW>::type M;
-            const M pm = node_positions<NW>(T, S, k, i);
+            const M pm = node_positions<NW, FM>(T, S, k, i);
             int Apre = 0, Bpre = 0, PMx = NEG_INF;
             M fwd = pm;
             while (fwd) {
@@ -962,8 +964,11 @@ __device__ __forceinline__ int bound_and_prune(const CtaTables& T, const WarpScr
     __syncwarp();
     if (!partial_ready) partial_schedule(T, S, f, b, k);
 
-    const bool both = srch.branch_mode > 0;
-    const bool fa = srch.find_all != 0;
+    // the fixed build (RULE != 0) serves searches without findAll, with the
+    // position tables present and the warp's free-position masks kept
+    const bool both = (RULE ? RULE : srch.branch_mode) > 0;
+    const bool fa = RULE ? false : srch.find_all != 0;
+    const bool masked = RULE || T.posj;
     int cbw[NW], cew[NW], cbs[NW], ces[NW];
 #pragma unroll
     for (int w = 0; w < NW; w++) { cbw[w] = 0; cew[w] = 0; cbs[w] = 0; ces[w] = 0; }
@@ -1081,13 +1086,13 @@ __device__ __forceinline__ int bound_and_prune(const CtaTables& T, const WarpScr
                     // the early exit lives in the runtime-options build only (SORT = 1):
                     // the default explorer passes a constant and keeps no trace of it
                     const int stop = (SORT && srch.early_stop) ? best : INT_MAX;
-                    if (T.posj) johnson_direct_masked<NW>(T, S, k, nc, cjob, cside, stop);
+                    if (masked) johnson_direct_masked<NW, (RULE != 0)>(T, S, k, nc, cjob, cside, stop);
                     else johnson_direct<NW>(T, S, um, nc, cjob, cside);
 #endif
                     cnt.direct_children += nc;
                     cnt.direct_free += (unsigned long long)nc * k;
                 } else {
-                    if (T.posj) johnson_sweep_masked<NW>(T, S, k, nF > 0, sF, nB > 0, sB);
+                    if (masked) johnson_sweep_masked<NW, (RULE != 0)>(T, S, k, nF > 0, sF, nB > 0, sB);
                     else johnson_children<NW>(T, S, um, nF > 0, sF, nB > 0, sB, nullptr);
                     cnt.sweeps++;
                     cnt.free_jobs += k;

@@ -682,7 +682,10 @@ int pbb_explore(pbb_engine* e, double seconds, int32_t* done)
         const unsigned long long budget = (unsigned long long)(win * 1e9);
         CK(cudaEventRecord(e->ev0, e->st));
         int variant = e->sample_d ? 2 : ((e->cfg.sorted_dfs || e->cfg.early_stop_johnson) ? 1 : 0);
-        if (variant == 0 && e->cfg.bounding_mode == 2 && e->cfg.branching_mode == 3) variant = 3;
+        // the fixed build also needs the per-warp masks in the launch
+        const bool masks = e->smem == pbbl::smem_bytes(e->H.n, e->H.m, e->H.Ppad, e->warps, 1);
+        if (variant == 0 && e->cfg.bounding_mode == 2 && e->cfg.branching_mode == 3 && !e->cfg.find_all && masks)
+            variant = 3;
         CK(pbbl::launch_explore(e->nw, e->group_d, e->ngroups_d, e->ctas, e->warps, e->smem, budget, e->max_rounds,
                                 e->select_budget, e->st, variant));
         CK(cudaEventRecord(e->ev1, e->st));

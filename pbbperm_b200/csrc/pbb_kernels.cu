@@ -237,7 +237,7 @@ __device__ __forceinline__ void record_solution(const DevGroup& G, const WarpScr
 // advance to the next unpruned node of the interval, evaluating leaves on the
 // way.  Returns 1 with a node to bound at R.line, 0 when the interval is
 // exhausted, 2 when the selection budget ran out (state stays consistent).
-template <int NW>
+template <int NW, int FM = 0>
 __device__ __forceinline__ int select_node(const DevGroup& G, const CtaTables& T, const WarpScratch& S, int id, Ivm<NW>& R,
                            int& best, WarpCounters& C, int budget)
 {
@@ -253,7 +253,7 @@ __device__ __forceinline__ int select_node(const DevGroup& G, const CtaTables& T
                 vset<NW>(R.pos, L, 0);
                 L--;
                 R.line = L;
-                if (S.fmask) fmask_flip(T, S, vget<NW>(R.pj, L));   // its job is free again
+                if (FM || S.fmask) fmask_flip(T, S, vget<NW>(R.pj, L));   // its job is free again
                 load_row<NW>(G.ivm, id, L, R.row);
                 load_path<NW>(G.ivm, id, L, R);
                 const int pp = vget<NW>(R.pos, L);
@@ -279,7 +279,7 @@ __device__ __forceinline__ int select_node(const DevGroup& G, const CtaTables& T
         C.decomposed++;
         const int u = vget<NW>(R.row, p);
         vset<NW>(R.pj, L, u);
-        if (S.fmask) fmask_flip(T, S, u);                  // u is fixed below this level
+        if (FM || S.fmask) fmask_flip(T, S, u);                  // u is fixed below this level
         path_down<NW>(T, R, u, vget<NW>(R.dir, L));
         int nr[NW];
 #pragma unroll
@@ -707,8 +707,8 @@ __global__ void pbb_root_kernel(const DevGroup* groups, int ngroups, const int* 
 // Persistent explorer loop.  Warp w of a group serves explorers w, w+W, ...
 // (W = warps of the group).  Runs until no explorer of the group holds work,
 // or `budget_ns` of device time has passed, or `max_rounds` rounds.  VAR = 3
-// is VAR 0 for boundingMode 2 with MinMin branching (the default search),
-// both compiled in as constants; VAR = 0
+// is VAR 0 for boundingMode 2 with MinMin branching and no findAll (the
+// default search), compiled in as constants; VAR = 0
 // compiles the sortedDFS row sorts, the early Johnson exit and node sampling
 // out of the hot loop; VAR = 1 follows each group's sortedDFS and
 // earlyStopJohnson settings; VAR = 2 also records sampled nodes into the
@@ -732,6 +732,12 @@ pbb_explore_kernel(const DevGroup* groups, const int* ngroups_d, int warps_per_c
     asm("mov.u32 %0, %%dynamic_smem_size;" : "=r"(dyn_smem));
     const int fm = G.inst.posj != nullptr &&
                    pbb_smem_plan(G.inst.n, G.inst.m, G.inst.Ppad, warps_per_cta, 1).total <= (int)dyn_smem;
+    if (VAR == 3 && !fm) {
+        // the fixed build relies on the masks; the host launches it only
+        // with room for them
+        if (threadIdx.x == 0) atomicOr(&G.ctl->status, PBB_ST_BADINPUT);
+        return;
+    }
     const SmemPlan sp = pbb_smem_plan(G.inst.n, G.inst.m, G.inst.Ppad, warps_per_cta, fm);
     CtaTables T;
     load_tables(G.inst, smem, sp, T);
@@ -811,7 +817,7 @@ pbb_explore_kernel(const DevGroup* groups, const int* ngroups_d, int warps_per_c
             // pay for the split, and keeps the donors splitting instead of
             // exploring
             if (since >= G.search.share_after && try_share<NW>(G, id, R) == 1) since = 0;
-            const int r = select_node<NW>(G, T, S, id, R, best, C, select_budget);
+            const int r = select_node<NW, (VAR == 3)>(G, T, S, id, R, best, C, select_budget);
             if (r == 1) since++;
             if (r == 1)
                 bound_current<NW, (VAR == 1 || VAR == 2), (VAR == 2), (VAR == 3 ? 3 : 0)>(G, T, S, id, R, mode, best, C);

@@ -16,7 +16,8 @@ cudaError_t launch_lower_ub(const DevGroup* groups, int g, int ub, cudaStream_t 
 // variant: 0 = no row sort, no early Johnson exit, no sampling (the hot
 // path); 1 = each group's sortedDFS / earlyStopJohnson settings; 2 = as 1 and
 // record sampled nodes (groups' SampleBuf); 3 = as 0 for groups that all
-// bound in mode 2 with MinMin branching (both compiled in)
+// bound in mode 2 with MinMin branching, without findAll, with position
+// tables (all compiled in)
 cudaError_t launch_explore(int nw, const DevGroup* groups, const int* ngroups_d, int ctas, int warps_per_cta, int smem,
                            unsigned long long budget_ns, int max_rounds, int select_budget, cudaStream_t st,
                            int variant = 0);

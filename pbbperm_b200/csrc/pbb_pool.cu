@@ -125,6 +125,7 @@ struct pbb_pool {
     cudaGraphExec_t window = nullptr;
     cudaGraphExec_t window_tail = nullptr;   // the same window with the tail's block shape
     cudaGraphExec_t window_fixed = nullptr, window_tail_fixed = nullptr;   // boundingMode 2 + MinMin builds
+    bool masks = false, tail_masks = false;   // launches sized with the per-warp free-position masks
     std::vector<Slot> slots;
     // the FIFO and the finished results are shared with submitting and
     // polling threads; everything else belongs to the thread driving step()
@@ -251,7 +252,10 @@ int pool_create(const pbb_pool_config* in, pbb_pool* P)
     {
         // per-warp free-position masks, when they cost no resident CTA
         const int ms = pbbl::smem_bytes(c.max_jobs, c.max_machines, P->Ppad_max, P->warps, 1);
-        if (ms <= optin && pbbl::explore_ctas_per_sm(P->nw, P->warps, ms) >= per_sm) P->smem = ms;
+        if (ms <= optin && pbbl::explore_ctas_per_sm(P->nw, P->warps, ms) >= per_sm) {
+            P->smem = ms;
+            P->masks = true;
+        }
     }
     // every window launches all the CTAs the GPU holds at once and spreads
     // them over the resident instances
@@ -265,11 +269,16 @@ int pool_create(const pbb_pool_config* in, pbb_pool* P)
         int ts = pbbl::smem_bytes(c.max_jobs, c.max_machines, P->Ppad_max, tw);
         const int tper = ts <= optin ? pbbl::explore_ctas_per_sm(P->nw, tw, ts) : 0;
         const int tms = pbbl::smem_bytes(c.max_jobs, c.max_machines, P->Ppad_max, tw, 1);
-        if (tper >= 1 && tms <= optin && pbbl::explore_ctas_per_sm(P->nw, tw, tms) >= tper) ts = tms;
+        bool tm = false;
+        if (tper >= 1 && tms <= optin && pbbl::explore_ctas_per_sm(P->nw, tw, tms) >= tper) {
+            ts = tms;
+            tm = true;
+        }
         if (tper >= 1) {
             P->tail_warps = tw;
             P->tail_smem = ts;
             P->tail_grid = sms * tper;
+            P->tail_masks = tm;
         }
     }
     // default explorer count: every warp of the widest grid owns one, so that
@@ -332,10 +341,11 @@ int pool_create(const pbb_pool_config* in, pbb_pool* P)
         return PBB_OK;
     };
     int rc = capture(P->grid, P->warps, P->smem, budget, 0, &P->window);
-    if (!rc) rc = capture(P->grid, P->warps, P->smem, budget, 3, &P->window_fixed);
+    if (!rc && P->masks) rc = capture(P->grid, P->warps, P->smem, budget, 3, &P->window_fixed);
     if (!rc && P->tail_warps > 0) {
         rc = capture(P->tail_grid, P->tail_warps, P->tail_smem, tail_budget, 0, &P->window_tail);
-        if (!rc) rc = capture(P->tail_grid, P->tail_warps, P->tail_smem, tail_budget, 3, &P->window_tail_fixed);
+        if (!rc && P->tail_masks)
+            rc = capture(P->tail_grid, P->tail_warps, P->tail_smem, tail_budget, 3, &P->window_tail_fixed);
     }
     if (rc) return rc;
     return PBB_OK;
@@ -559,8 +569,11 @@ extern "C" int pbb_pool_step(pbb_pool* P, int32_t* resident, int32_t* queued)
     PCK(cudaMemcpyAsync(P->ngroups_d, &nact, sizeof(int), cudaMemcpyHostToDevice, P->st), "upload");
     bool fixed = true;
     for (int i = 0; i < nact; i++)
-        fixed = fixed && act[i].search.bound_mode == 2 && act[i].search.branch_mode == 3;
-    cudaGraphExec_t win = tail ? (fixed ? P->window_tail_fixed : P->window_tail) : (fixed ? P->window_fixed : P->window);
+        fixed = fixed && act[i].search.bound_mode == 2 && act[i].search.branch_mode == 3 && !act[i].search.find_all &&
+                act[i].inst.posj != nullptr;
+    cudaGraphExec_t win = tail ? P->window_tail : P->window;
+    if (fixed && tail && P->window_tail_fixed) win = P->window_tail_fixed;
+    if (fixed && !tail && P->window_fixed) win = P->window_fixed;
     if (nact > 0) PCK(cudaGraphLaunch(win, P->st), "window launch");
     PCK(cudaStreamSynchronize(P->st), "window");
     // retire the finished instances
