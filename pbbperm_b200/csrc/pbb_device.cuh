@@ -914,8 +914,8 @@ __device__ __forceinline__ int choose_dir(int rule, int line, int ub, const int 
 }
 
 struct NodeCounters {
-    unsigned long long simple, johnson;
-    unsigned long long sweeps, free_jobs, swept_children, direct_children, direct_free;
+    unsigned simple, johnson;
+    unsigned sweeps, free_jobs, swept_children, direct_children, direct_free;
 };
 
 // Bound the children of the node whose free jobs are `row[0..k)` (front and
@@ -1090,7 +1090,7 @@ __device__ __forceinline__ int bound_and_prune(const CtaTables& T, const WarpScr
                     else johnson_direct<NW>(T, S, um, nc, cjob, cside);
 #endif
                     cnt.direct_children += nc;
-                    cnt.direct_free += (unsigned long long)nc * k;
+                    cnt.direct_free += (unsigned)(nc * k);
                 } else {
                     if (masked) johnson_sweep_masked<NW, (RULE != 0)>(T, S, k, nF > 0, sF, nB > 0, sB);
                     else johnson_children<NW>(T, S, um, nF > 0, sF, nB > 0, sB, nullptr);

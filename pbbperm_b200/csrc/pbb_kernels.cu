@@ -203,10 +203,28 @@ __device__ __forceinline__ void build_lists(const WarpScratch& S, const Ivm<NW>&
     __syncwarp();
 }
 
+// 32-bit per warp (fewer live registers in the explorer loop), added to the
+// group's 64-bit counters at least every 2^20 decomposed nodes
 struct WarpCounters {
-    unsigned long long decomposed, simple, johnson, leaves;
-    unsigned long long sweeps, free_jobs, swept_children, direct_children, direct_free;
+    unsigned decomposed, simple, johnson, leaves;
+    unsigned sweeps, free_jobs, swept_children, direct_children, direct_free;
 };
+
+__device__ __forceinline__ void flush_counters(const DevGroup& G, WarpCounters& C)
+{
+    if (lane_id() == 0) {
+        atomicAdd(&G.ctl->decomposed, (unsigned long long)C.decomposed);
+        atomicAdd(&G.ctl->simple_bounds, (unsigned long long)C.simple);
+        atomicAdd(&G.ctl->johnson_bounds, (unsigned long long)C.johnson);
+        atomicAdd(&G.ctl->leaves, (unsigned long long)C.leaves);
+        atomicAdd(&G.ctl->jsweeps, (unsigned long long)C.sweeps);
+        atomicAdd(&G.ctl->jfree, (unsigned long long)C.free_jobs);
+        atomicAdd(&G.ctl->jchild, (unsigned long long)C.swept_children);
+        atomicAdd(&G.ctl->jdirect, (unsigned long long)C.direct_children);
+        atomicAdd(&G.ctl->jdirect_free, (unsigned long long)C.direct_free);
+    }
+    C = WarpCounters{0, 0, 0, 0, 0, 0, 0, 0, 0};
+}
 
 // Record an improving leaf: permutation into the explorer's slot, then the
 // (cost, explorer) key into the group's best (solution.cpp:27-45 restated as
@@ -382,13 +400,13 @@ __device__ __forceinline__ void bound_current(const DevGroup& G, const CtaTables
                                                     true, rec);
     vset<NW>(R.dir, L, d);
     store_row<NW>(G.ivm, id, L, R.row);
-    C.simple += nc.simple;
-    C.johnson += nc.johnson;
-    C.sweeps += nc.sweeps;
-    C.free_jobs += nc.free_jobs;
-    C.swept_children += nc.swept_children;
-    C.direct_children += nc.direct_children;
-    C.direct_free += nc.direct_free;
+    C.simple += (unsigned)nc.simple;
+    C.johnson += (unsigned)nc.johnson;
+    C.sweeps += (unsigned)nc.sweeps;
+    C.free_jobs += (unsigned)nc.free_jobs;
+    C.swept_children += (unsigned)nc.swept_children;
+    C.direct_children += (unsigned)nc.direct_children;
+    C.direct_free += (unsigned)nc.direct_free;
 }
 
 // ---------------------------------------------------------------------------
@@ -822,6 +840,7 @@ pbb_explore_kernel(const DevGroup* groups, const int* ngroups_d, int warps_per_c
             if (r == 1)
                 bound_current<NW, (VAR == 1 || VAR == 2), (VAR == 2), (VAR == 3 ? 3 : 0)>(G, T, S, id, R, mode, best, C);
             worked = true;
+            if (C.decomposed >= (1u << 20)) flush_counters(G, C);
             if (r == 0) {
                 // interval exhausted: leave the pool of busy explorers (the
                 // registers need not go back: nobody resumes this interval)
@@ -857,17 +876,7 @@ pbb_explore_kernel(const DevGroup* groups, const int* ngroups_d, int warps_per_c
         }
     }
     if (cached >= 0) store_ivm<NW>(G.ivm, cached, R);
-    if (lane_id() == 0) {
-        atomicAdd(&G.ctl->decomposed, C.decomposed);
-        atomicAdd(&G.ctl->simple_bounds, C.simple);
-        atomicAdd(&G.ctl->johnson_bounds, C.johnson);
-        atomicAdd(&G.ctl->leaves, C.leaves);
-        atomicAdd(&G.ctl->jsweeps, C.sweeps);
-        atomicAdd(&G.ctl->jfree, C.free_jobs);
-        atomicAdd(&G.ctl->jchild, C.swept_children);
-        atomicAdd(&G.ctl->jdirect, C.direct_children);
-        atomicAdd(&G.ctl->jdirect_free, C.direct_free);
-    }
+    flush_counters(G, C);
 }
 
 // Lower a group's incumbent to `ub` (bound found elsewhere, no permutation here).
