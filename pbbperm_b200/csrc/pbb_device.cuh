@@ -25,7 +25,7 @@
 // a lone child gets its own one-chain direct scan (instead of two chains, one
 // repeating the other)
 #ifndef PBB_DIRECT_ONE
-#define PBB_DIRECT_ONE 0
+#define PBB_DIRECT_ONE 1
 #endif
 // unroll factor of the loop that builds a pair's free-position mask
 #ifndef PBB_FREEPOS_UNROLL
