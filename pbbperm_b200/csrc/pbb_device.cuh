@@ -1083,9 +1083,12 @@ __device__ __forceinline__ int bound_and_prune(const CtaTables& T, const WarpScr
                             }
                         }
                     }
-                    // the early exit lives in the runtime-options build only (SORT = 1):
-                    // the default explorer passes a constant and keeps no trace of it
-                    const int stop = (SORT && srch.early_stop) ? best : INT_MAX;
+                    // early exit: in the runtime-options build (SORT = 1) when
+                    // earlyStopJohnson asks for it; in the default search's build
+                    // (RULE != 0) always -- it only changes the values of
+                    // children that are pruned anyway, which that build never
+                    // reports; the general hot build keeps no trace of it
+                    const int stop = RULE ? best : ((SORT && srch.early_stop) ? best : INT_MAX);
                     if (masked) johnson_direct_masked<NW, (RULE != 0)>(T, S, k, nc, cjob, cside, stop);
                     else johnson_direct<NW>(T, S, um, nc, cjob, cside);
 #endif
