@@ -94,6 +94,26 @@ def test_counters_50x20_below_optimum(mode):
         assert got[k] == want[k], (k, got[k], want[k])
 
 
+def test_counters_64_jobs_without_kept_masks():
+    """64 jobs x 20 machines: the tables leave no room for the per-warp
+    free-position masks at the largest warp count, so the engine runs the
+    general explorer build, which rebuilds each pair's mask at every node.
+    UB = 4421 lies below every schedule (the oracle finds none), so the
+    search is deterministic: counters equal the oracle's."""
+    import torch
+    p = synthetic_instance(5, 64, 20)
+    want = Oracle(p).solve(4421, bound_mode=2)
+    assert want["complete"] and not want["found"] and want["decomposed"] > 10000
+    sms = torch.cuda.get_device_properties(0).multi_processor_count
+    with pb.Engine(p, pb.Config(nbIVMs=16384, boundingMode=2)) as e:
+        got = e.solve(ub=4421)
+        warps = e.kernel_stats()["warps"]          # all CTAs' warps; one CTA per SM
+    assert warps // sms < 20, (warps, sms)
+    assert got["complete"] and not got["found"]
+    for k in KEYS:
+        assert got[k] == want[k], (k, got[k], want[k])
+
+
 @pytest.mark.parametrize("ivms", [1, 3, 64, 4096, 65536])
 def test_counters_independent_of_explorer_count(ivms):
     p = synthetic_instance(24, 13, 20)
