@@ -2,6 +2,7 @@
 import ctypes
 import os
 import re
+import subprocess
 
 import numpy as np
 import pytest
@@ -87,3 +88,36 @@ def test_vrf_roundtrip(tmp_path):
     path = str(tmp_path / "VTEST_Gap.txt")
     write_vrf(path, p)
     assert (read_vrf(path) == p).all()
+
+
+STRUCTS = [("pbb_instance", "_Instance"), ("pbb_config", "_Config"), ("pbb_stats", "_Stats"),
+           ("pbb_result", "_Result"), ("pbb_work", "_Work"), ("pbb_pool_config", "_PoolConfig"),
+           ("pbb_pool_result", "_PoolResult"), ("pbb_bound_out", "_BoundOut")]
+
+
+def test_python_struct_mirrors_match_the_c_headers(tmp_path):
+    """Every ctypes mirror in pbbperm_b200 has the C struct's size and each
+    field's offset, as gcc lays them out from include/*.h."""
+    lines = ['#include <stdio.h>', '#include <stddef.h>', '#include "pbbperm.h"', '#include "pbbperm_diag.h"',
+             'int main(void) {']
+    for c_name, py_name in STRUCTS:
+        S = getattr(pb, py_name)
+        lines.append('printf("%s size %%zu\\n", sizeof(%s));' % (c_name, c_name))
+        for f in S._fields_:
+            lines.append('printf("%s %s %%zu\\n", offsetof(%s, %s));' % (c_name, f[0], c_name, f[0]))
+    lines += ['return 0;', '}']
+    src = tmp_path / "layout.c"
+    src.write_text("\n".join(lines))
+    exe = tmp_path / "layout"
+    subprocess.run(["gcc", "-std=c99", "-I", os.path.join(ROOT, "include"), str(src), "-o", str(exe)], check=True)
+    out = subprocess.run([str(exe)], capture_output=True, text=True, check=True).stdout.split("\n")
+    got = {}
+    for line in out:
+        if line:
+            a, b, v = line.split()
+            got[(a, b)] = int(v)
+    for c_name, py_name in STRUCTS:
+        S = getattr(pb, py_name)
+        assert got[(c_name, "size")] == ctypes.sizeof(S), c_name
+        for f in S._fields_:
+            assert got[(c_name, f[0])] == getattr(S, f[0]).offset, (c_name, f[0])
