@@ -63,6 +63,8 @@ def parse():
     ap.add_argument("--pool-window", type=float, default=0.0,
                     help="device time per pool window (batch; 0: the autotuner's choice)")
     ap.add_argument("--config2", type=int, default=1, help="add the 20x20 solve-to-completion sub-object (N=1)")
+    ap.add_argument("--mode1", type=int, default=1,
+                    help="add the 50x20 Johnson-only (boundingMode 1) sub-object (N=1)")
     ap.add_argument("--summary-batch", type=int, default=128,
                     help="add a compact batched sub-object over this many instances (0: none; N=1)")
     ap.add_argument("--summary-serve", type=int, default=200,
@@ -340,6 +342,8 @@ def run_ours(args):
         extra = {}
         if ws == 1 and args.config2:
             extra["config2"] = run_config2(local)
+        if ws == 1 and args.mode1:
+            extra["mode1"] = run_mode1(local)
         if ws == 1 and args.summary_batch > 0:
             extra["batch"] = compact_batch(args.summary_batch, local)
         if ws == 1 and args.summary_serve > 0:
@@ -396,6 +400,32 @@ def run_config2(device):
             "decomposed": best["decomposed"], "complete": all(r["complete"] for r in runs),
             "counters_equal_reference": exact, "runs": len(runs),
             "device_seconds_all": [round(r["device_seconds"], 4) for r in runs]}
+
+
+def run_mode1(device, windows=3, window_s=2.0):
+    """The bench workload with the Johnson bound on every child (boundingMode
+    1: no weak pre-filter, the side chosen on the Johnson values), MinMin,
+    UB = NEH, 65,536 explorers: decomposed nodes/s and Johnson bounds/s over
+    fixed device-time windows after one warm-up window."""
+    import pbbperm_b200 as pb
+    p = pb.synthetic_instance(SEED, N_JOBS, N_MACH)
+    ub = pb.neh(p)[0]
+    cfg = pb.Config(boundingMode=1, adaptiveBranchingMode=BRANCH_MODE, nbIVMs=NB_IVMS, device=device)
+    with pb.Engine(p, cfg) as e:
+        e.start(ub=ub)
+        e.explore(window_s)
+        r0 = e.result()
+        for _ in range(windows):
+            e.explore(window_s)
+        r1 = e.result()
+    dt = r1["device_seconds"] - r0["device_seconds"]
+    nodes = r1["decomposed"] - r0["decomposed"]
+    jb = r1["johnson_bounds"] - r0["johnson_bounds"]
+    return {"workload": "pfsp-50x20-u1-99-seed2, boundingMode 1 (Johnson on every child), MinMin, UB = NEH, "
+                        "65536 explorers, %d x %.0f s windows" % (windows, window_s),
+            "nodes_per_s": round(nodes / dt, 1) if dt > 0 else None,
+            "johnson_bounds_per_s": round(jb / dt, 1) if dt > 0 else None,
+            "device_seconds": round(dt, 3)}
 
 
 # the pool shape the autotuner picks on the batched workload (bench.py

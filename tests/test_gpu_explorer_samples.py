@@ -33,8 +33,8 @@ def minmin_side(cb, ce, ub):
     return np.where(cnt > 0, 1, np.where(cnt < 0, 0, np.where(elim > 0, 0, 1)))
 
 
-def collect(p, ub, ivms, cap, rate_log2, warm_s):
-    with pb.Engine(p, pb.Config(boundingMode=2, adaptiveBranchingMode=3, nbIVMs=ivms)) as e:
+def collect(p, ub, ivms, cap, rate_log2, warm_s, mode=2):
+    with pb.Engine(p, pb.Config(boundingMode=mode, adaptiveBranchingMode=3, nbIVMs=ivms)) as e:
         e.start(ub=ub)
         done = e.explore(warm_s) if warm_s > 0 else False
         e.sample_nodes(cap, rate_log2)
@@ -95,3 +95,39 @@ def test_explorer_sampled_nodes_match_reference_bounds(n, m, seed, ivms, cap, ra
     # the sample spans the tree: many depths and both scan regimes
     assert len(np.unique(s["line"])) >= 10
     assert checked > 0
+
+
+def test_explorer_sampled_nodes_johnson_only_mode():
+    """boundingMode 1 on the bench instance: the explorer evaluates the
+    Johnson bound of every free child on both sides (computeStrongBounds
+    without the weak pre-filter, ivm_bound.cpp:141-195), chooses the side by
+    MinMin on those values, and each value equals the reference library's."""
+    n, m = 50, 20
+    p = synthetic_instance(2, n, m)
+    ub = pb.neh(p)[0]
+    s = collect(p, ub, 65536, 10000, 6, 0.5, mode=1)
+    cnt = len(s["k"])
+    assert cnt >= 10000, cnt
+    sched, l1, l2 = s["sched"], s["limit1"], s["limit2"]
+    assert (np.sort(sched, axis=1) == np.arange(n)).all()
+    sb, se = s["strong_begin"], s["strong_end"]
+    free = np.zeros((cnt, n), bool)
+    for i in range(cnt):
+        free[i, sched[i, l1[i] + 1:l2[i]]] = True
+    assert ((sb != 0) == free).all() and ((se != 0) == free).all()
+    assert (s["weak_begin"] == 0).all() and (s["weak_end"] == 0).all()
+    assert (s["side"] == minmin_side(sb, se, s["best"])).all()
+    if oracle.reference_available():
+        _, _, rsb, rse = oracle.Reference(p).children_batch(sched, l1, l2, free, free)
+        idx = np.arange(cnt)
+    else:
+        O = Oracle(p)
+        idx = np.arange(0, cnt, max(1, cnt // 500))
+        rsb, rse = np.zeros((cnt, n), np.int32), np.zeros((cnt, n), np.int32)
+        for i in idx:
+            rsb[i] = np.where(free[i], O.strong_children(sched[i], l1[i], l2[i], True), 0)
+            rse[i] = np.where(free[i], O.strong_children(sched[i], l1[i], l2[i], False), 0)
+    for name, got, want in (("strong_begin", sb, rsb), ("strong_end", se, rse)):
+        bad = idx[(got[idx] != want[idx]).any(axis=1)]
+        assert len(bad) == 0, (name, len(bad), bad[:5].tolist())
+    assert len(np.unique(s["line"])) >= 10
