@@ -288,14 +288,17 @@ __device__ __forceinline__ int select_node(const DevGroup& G, const CtaTables& T
             }
             continue;
         }
-        const int c = next_open_cell<NW>(R.row, p, k);   // goRight over pruned cells
-        if (c != p) {
-            vset<NW>(R.pos, L, c);
-            continue;
+        int q = next_open_cell<NW>(R.row, p, k);         // goRight over pruned cells
+        if (q != p) {
+            vset<NW>(R.pos, L, q);
+            // an open cell was found: go down into it in this same step, as
+            // the next iteration would (the interval end is checked again)
+            if (q >= k) continue;
+            if (!before_end<NW>(R.pos, R.end, n)) return 0;
         }
-        // goDown (ivm.cpp:73-104): the node at (L, p) is decomposed
+        // goDown (ivm.cpp:73-104): the node at (L, q) is decomposed
         C.decomposed++;
-        const int u = vget<NW>(R.row, p);
+        const int u = vget<NW>(R.row, q);
         vset<NW>(R.pj, L, u);
         if (FM || S.fmask) fmask_flip(T, S, u);                  // u is fixed below this level
         path_down<NW>(T, R, u, vget<NW>(R.dir, L));
@@ -303,7 +306,7 @@ __device__ __forceinline__ int select_node(const DevGroup& G, const CtaTables& T
 #pragma unroll
         for (int w = 0; w < NW; w++) {
             const int idx = w * 32 + lane_id();
-            int src = idx < p ? idx : idx + 1;
+            int src = idx < q ? idx : idx + 1;
             if (src >= 32 * NW) src = 0;
             nr[w] = cell_job(vgather<NW>(R.row, src));
         }
