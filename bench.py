@@ -34,8 +34,8 @@ N_JOBS, N_MACH, SEED = 50, 20, 2
 NB_IVMS = 65536
 # explorer-kernel DRAM traffic (read + write) per second of window, from
 # `ncu --set full` on this workload (dram__bytes_read.sum + dram__bytes_write.sum
-# = 14.07 MB + 4.55 MB over a 50.1 ms launch)
-NCU_DRAM_BYTES_PER_S = (14.066688e6 + 4.546048e6) / 0.050125536
+# = 14.43 MB + 4.51 MB over a 50.1 ms launch)
+NCU_DRAM_BYTES_PER_S = (14.431488e6 + 4.507392e6) / 0.050098560
 BOUND_MODE, BRANCH_MODE = 2, 3
 METRIC = "decomposed nodes/s (50x20, Johnson LB)"
 
